@@ -1,0 +1,379 @@
+"""Benchmark: time to relative residual 1e-8 on 3D linear elasticity, 128^3 nodes.
+
+Workload (one step = one full solve): 3D linear elasticity on a 128^3-node
+structured hex8 mesh (E = 1, nu = 0.3, face x = 0 clamped, body force with a
+seeded perturbation), block CSR with ndof = 3 (2,097,152 block rows,
+55,742,968 3x3 blocks), CG + DIAG (3x3 block Jacobi), relative residual
+sqrt(<r,r>/<r0,r0>) < 1e-8. Inputs are synthetic (monolis_b200.problems).
+
+Our arm: the FP32-inner / FP64-refined CG (headline `value`, device-resident
+b and x), the plain FP64 CG beside it, standalone SpMV roofline figures, and
+`e2e` = the same solve through monolis_solve_R with host b/x (pinned), which
+includes uploading the matrix (the library re-uploads by default).
+`--impl reference`: the CPU oracle (restatement of the reference's CG) on the
+host cores, timed on a bounded sample of iterations and extrapolated to the
+oracle's iteration count for this system.
+Multi-GPU: independent replicas (one system per rank, weak scaling), time =
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from monolis_b200 import api, problems  # noqa: E402
+
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libmonolis_oracle.so")
+FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")
+METRIC = "time to rel.res 1e-8, FP32-refined block-CSR CG (3D elasticity 128^3 nodes, ndof=3)"
+TOL = 1e-8
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": 0}
+        busy = [s for s in sm if s > 0.5 * (smax or max(sm))] or sm
+        return {"sm_mhz": float(np.median(busy)), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def oracle_iterations(n):
+    try:
+        with open(FIXTURE) as f:
+            d = json.load(f)
+        return d.get(f"elasticity_n{n}_cg_diag_tol1e-08")
+    except (OSError, ValueError):
+        return None
+
+
+def run_reference(args, rank):
+    """CPU oracle on the host cores: bounded sample, extrapolated."""
+    if rank != 0:
+        return
+    orc = api.load_library(ORACLE_SO, oracle=True)
+    threads = os.cpu_count() or 1
+    orc.oracle_set_threads(threads)
+    m = api.Monolis(orc)
+    t0 = time.perf_counter()
+    b = problems.elasticity(m, n=args.n)
+    t_asm = time.perf_counter() - t0
+    m.quiet()
+    m.set_error_abort(False)
+    m.set_method(api.ITER_CG)
+    m.set_precond(api.PREC_DIAG)
+    m.set_tolerance(TOL)
+    it_full = oracle_iterations(args.n)
+    sample_iters = args.cpu_sample_iters
+    m.set_maxiter(sample_iters)
+    per_step = []
+    for k in range(args.warmup + args.steps):
+        x = np.zeros_like(b)
+        t1 = time.perf_counter()
+        m.solve(b, x)
+        dt = time.perf_counter() - t1
+        if k >= args.warmup:
+            per_step.append(dt)
+    t_sample = float(np.median(per_step))
+    t_iter = t_sample / sample_iters
+    iters = it_full if it_full else None
+    value = t_iter * iters if iters else None
+    line = {
+        "impl": "reference", "metric": METRIC.replace("FP32-refined", "FP64 CPU oracle"), "value": value,
+        "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": value * 1e3 if value else None, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"3D elasticity {args.n}^3 nodes hex8 ndof=3, CG+DIAG, rel.res 1e-8",
+                   "parallelism": "cpu"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
+                         "sample": f"{sample_iters} CG iterations per step (median of {args.steps}), "
+                                   f"extrapolated x {iters} iterations (oracle count for this system)"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "assembly_s": t_asm, "s_per_iteration": t_iter, "oracle_iterations": iters,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128)
+    ap.add_argument("--cpu-sample-iters", type=int, default=10)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    lib = api.load_product()
+    m = api.Monolis(lib)
+    t0 = time.perf_counter()
+    b = problems.elasticity(m, n=args.n)
+    t_asm = time.perf_counter() - t0
+    m.quiet()
+    m.set_error_abort(False)
+    m.set_method(api.ITER_CG)
+    m.set_precond(api.PREC_DIAG)
+    m.set_tolerance(TOL)
+    m.set_maxiter(20000)
+    N, nd, nz = m.N, m.NDOF, m.NZ
+    n_unk = N * nd
+    log(f"[rank {rank}] assembled n={args.n}: N={N} nz={nz} in {t_asm:.1f}s")
+
+    stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros(n_unk, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+
+    def timed_solve(precision):
+        m.set_precision(precision)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = m.device_solve(d_b.data_ptr(), d_x.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        if rc not in (0,):
+            raise RuntimeError(f"solve failed: {api.STATUS_NAMES.get(rc, rc)}")
+        return e0.elapsed_time(e1) * 1e-3, m.get_converge_iter(), m.get_converge_residual()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # FP64 plain solver (reference semantics on the GPU); the device matrix is
+    # kept between the device-resident solves
+    m.set_matrix_cache(True)
+    m.set_precision(0)
+    m.device_prepare()
+    t64, it64, res64 = timed_solve(0)
+    t64, it64, res64 = timed_solve(0)
+    x64 = d_x.clone()
+    # mixed precision: warmup then timed steps
+    m.set_precision(1)
+    m.device_prepare()
+    for _ in range(args.warmup):
+        timed_solve(1)
+    times, iters = [], []
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t, it, res = timed_solve(1)
+            times.append(t)
+            iters.append(it)
+            launches += int(m.Iarray[36])
+    barrier()
+    clocks = clk.summary()
+    t_mixed = float(np.mean(times))
+    nref = int(m.Iarray[api.B200_PRM_I_N_REFINE])
+    err_vs_fp64 = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
+    # true FP64 residual of the mixed solution (device FP64 SpMV)
+    d_r = torch.empty_like(d_x)
+    m.device_matvec(d_x.data_ptr(), d_r.data_ptr())
+    stream.synchronize()
+    r0 = torch.linalg.norm(d_b).item()  # x0 = 0: r0 = b
+    true_res = torch.linalg.norm(d_b - d_r).item() / r0
+
+    # SpMV roofline (standalone kernels, FP64 and FP32), CUDA events on the library stream
+    nzb, padded, nslices = m.device_info()
+    xs64 = torch.randn(n_unk, dtype=torch.float64, device="cuda")
+    ys64 = torch.empty_like(xs64)
+    xs32 = xs64.float()
+    ys32 = torch.empty_like(xs32)
+    torch.cuda.synchronize()
+    spmv = {}
+    reps = 20
+    for name, fp32, xs, ys, vb in (("fp64", False, xs64, ys64, 8), ("fp32", True, xs32, ys32, 4)):
+        for _ in range(3):
+            m.device_matvec(xs.data_ptr(), ys.data_ptr(), fp32=fp32)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            m.device_matvec(xs.data_ptr(), ys.data_ptr(), fp32=fp32)
+        e1.record(stream)
+        e1.synchronize()
+        dt = e0.elapsed_time(e1) * 1e-3 / reps
+        byts = problems.spmv_bytes(nz, N, nd, vb)
+        spmv[name] = {"seconds": dt, "bytes": byts, "gbs": byts / dt / 1e9}
+    peak, peak_kind = measured_peak()
+
+    # e2e through monolis_solve_R with pinned host buffers (matrix upload included)
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.zeros(n_unk, dtype=torch.float64).pin_memory()
+    m.set_matrix_cache(False)
+    m.set_precision(1)
+    e2e_times = []
+    for k in range(1 + args.steps):
+        hx.zero_()
+        t1 = time.perf_counter()
+        m.solve(hb.numpy(), hx.numpy())
+        dt = time.perf_counter() - t1
+        if k >= 1:
+            e2e_times.append(dt)
+    t_e2e = float(np.mean(e2e_times))
+    h2d = nz * nd * nd * 8 + nz * 4 + (N + 1) * 4 + n_unk * 8  # values, items, offsets, b
+    d2h = n_unk * 8
+
+    # max over ranks
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
+    t_mixed_max = max_over_ranks(t_mixed)
+    t64_max = max_over_ranks(t64)
+    t_e2e_max = max_over_ranks(t_e2e)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            orc = api.load_library(ORACLE_SO, oracle=True)
+            threads = os.cpu_count() or 1
+            orc.oracle_set_threads(threads)
+            mo = api.Monolis(orc)
+            ind = m.csr_index().copy()
+            item0 = (m.csr_item() - 1).astype(np.int32)
+            mo.set_matrix_BCSR(N, N, nd, nz, m.values(), ind, item0)
+            mo.quiet()
+            mo.set_error_abort(False)
+            mo.set_method(api.ITER_CG)
+            mo.set_precond(api.PREC_DIAG)
+            mo.set_maxiter(args.cpu_sample_iters)
+            xo = np.zeros_like(b)
+            t1 = time.perf_counter()
+            mo.solve(b, xo)
+            t_s = time.perf_counter() - t1
+            t_it = t_s / args.cpu_sample_iters
+            cpu = {"value": t_it * it64, "unit": "s", "cores": threads, "kind": "port",
+                   "sample": f"{args.cpu_sample_iters} oracle CG iterations on the same system "
+                             f"({t_s:.2f} s), extrapolated x {it64} iterations"}
+            mo.finalize()
+        except Exception as e:  # report, do not hide
+            cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        dom = spmv["fp32"]
+        line = {
+            "metric": METRIC, "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
+            "config": {"workload": f"3D linear elasticity {args.n}^3 nodes, hex8 Q1, E=1 nu=0.3, ndof=3, "
+                                   f"{nz} 3x3 blocks, CG + 3x3 block-Jacobi, rel.res 1e-8",
+                       "unknowns": n_unk, "nz_blocks": nz, "padded_blocks": padded,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (matrix 4.3 GB FP64 + 2.3 GB FP32)"},
+            "iterations": int(np.median(iters)), "fp64_refreshes": nref, "true_rel_residual": true_res,
+            "rel_error_vs_fp64_solution": err_vs_fp64,
+            "fp64": {"value": t64_max, "unit": "s", "iterations": it64, "rel_residual": res64},
+            "speedup_vs_fp64": t64_max / t_mixed_max,
+            "spmv": {k: {"gbs": v["gbs"], "us": v["seconds"] * 1e6, "bytes": v["bytes"],
+                         "frac_of_measured": v["gbs"] / peak, "frac_of_8tbs": v["gbs"] / 8000.0}
+                     for k, v in spmv.items()},
+            "roofline": {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": dom["gbs"] / peak, "traffic": None,
+                         "kernel": "FP32 sliced-ELL block SpMV (ndof 3), standalone launch",
+                         "peak_kind": peak_kind},
+            "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "assembly_s": t_asm,
+        }
+        print(json.dumps(line), flush=True)
+    m.finalize()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

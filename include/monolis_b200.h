@@ -1,0 +1,97 @@
+/* monolis_b200.h -- entry points that libmonolis_b200.so adds to the monolis
+ * C API (include/monolis.h). None of them has a counterpart in the reference
+ * library unless its comment cites one; they expose what the reference keeps
+ * internal (device residency, precision) and the added solver forms.
+ *
+ * All functions return 0 on success or a MONOLIS_B200_* status code; the
+ * same code is written to mat->prm.Iarray[MONOLIS_PRM_I_IERR] by solves.
+ */
+#ifndef MONOLIS_B200_H
+#define MONOLIS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#include <stdbool.h>
+#include "monolis.h"
+
+/* ---- status codes (Iarray[MONOLIS_PRM_I_IERR]; the reference leaves it at -1) ---- */
+static const int MONOLIS_B200_OK         = 0;
+static const int MONOLIS_B200_MAXITER    = 1; /* max_iter reached without convergence */
+static const int MONOLIS_B200_BREAKDOWN  = 2; /* BiCGSTAB: rho or (RT,V) exactly zero */
+static const int MONOLIS_B200_NONFINITE  = 3; /* residual became NaN/Inf */
+static const int MONOLIS_B200_TIMEOUT    = 4; /* device loop gave no verdict */
+static const int MONOLIS_B200_BAD_INPUT  = 5; /* unsupported method/precond/ndof or bad arrays */
+static const int MONOLIS_B200_CUDA_ERROR = 6;
+
+/* ---- added parameter slots (indices the reference leaves unused, >= 30) ---- */
+static const int MONOLIS_B200_PRM_I_PRECISION      = 30; /* 0: FP64 (default), 1: FP32 inner + FP64 refinement */
+static const int MONOLIS_B200_PRM_I_MATRIX_CACHE   = 31; /* 1: reuse the device matrix while MATRIX_VERSION is unchanged */
+static const int MONOLIS_B200_PRM_I_MATRIX_VERSION = 32; /* bumped by every matrix-mutating call of this library */
+static const int MONOLIS_B200_PRM_I_N_REFINE       = 33; /* out: FP64 residual refreshes of the mixed solver */
+static const int MONOLIS_B200_PRM_I_BATCH          = 34; /* iterations per graph launch (0: 16) */
+static const int MONOLIS_B200_PRM_I_CHECK          = 35; /* 1: validate CSR index/item before upload */
+static const int MONOLIS_B200_PRM_I_LAUNCHES       = 36; /* out: kernels launched by the last solve */
+
+static const int MONOLIS_B200_PRM_R_REFINE_DELTA   = 30; /* refresh when ||r|| < delta*max||r|| (0: 0.1) */
+static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */
+static const int MONOLIS_B200_PRM_R_TIME_D2H       = 32; /* out: seconds spent on device->host copies */
+static const int MONOLIS_B200_PRM_R_TIME_LOOP      = 33; /* out: seconds in the device iteration loop */
+
+static const int MONOLIS_B200_PRECISION_FP64  = 0;
+static const int MONOLIS_B200_PRECISION_MIXED = 1;
+
+/* Precision of the Krylov loop. MIXED keeps values and vectors in FP32 inside
+ * the loop, accumulates every dot product and the alpha/beta recurrences in
+ * FP64, and refreshes an FP64 solution with an FP64 residual r = b - A x. */
+int monolis_b200_set_precision(MONOLIS* mat, int precision);
+
+/* Keep the device copy of the matrix between solves. Only calls of this
+ * library that change the matrix invalidate it; a caller that writes
+ * mat->mat.R.A directly must call monolis_b200_matrix_changed(). */
+void monolis_b200_set_matrix_cache(MONOLIS* mat, bool enable);
+void monolis_b200_matrix_changed(MONOLIS* mat);
+
+/* ---- bulk host assembly ---- */
+
+/* get_nonzero_pattern_by_simple_mesh_R with a flat element array
+ * elem[e*n_base + a] (0-based); same resulting CSR as the int** form. */
+int monolis_b200_get_nonzero_pattern_by_simple_mesh_flat_R(
+  MONOLIS* mat, int n_node, int n_base, int n_dof, int n_elem, const int* elem);
+
+/* Element-by-element monolis_add_matrix_to_sparse_matrix_R for n_elem
+ * elements: element e adds scale[e] * val[e*val_stride + k] (row-major,
+ * (n_base*ndof)^2 entries). scale may be NULL (1.0); val_stride 0 means all
+ * elements share one matrix. Result is bit-identical to the calls made one
+ * element at a time in order. */
+int monolis_b200_add_elements_R(
+  MONOLIS* mat, int n_elem, int n_base, const int* elem, const double* val,
+  long long val_stride, const double* scale);
+
+/* ---- device residency (device pointers; work is ordered on the library's
+ * stream, monolis_b200_stream()) ---- */
+
+/* Stream on which every device entry point of this library runs (cudaStream_t). */
+void* monolis_b200_stream(void);
+
+/* Upload the matrix, build the device layout and the DIAG factors (and the
+ * FP32 copies when the precision parameter is MIXED). */
+int monolis_b200_device_prepare(MONOLIS* mat);
+
+/* Solve with b and x in device memory, using the prepared device matrix.
+ * Synchronous; fills CUR_ITER, CUR_RESID, IERR and the timing slots. */
+int monolis_b200_device_solve_R(MONOLIS* mat, const double* d_b, double* d_x);
+
+/* y = A x with device vectors (asynchronous on the library stream). */
+int monolis_b200_device_matvec_R(MONOLIS* mat, const double* d_x, double* d_y);
+int monolis_b200_device_matvec_R32(MONOLIS* mat, const float* d_x, float* d_y);
+
+/* Layout facts of the prepared device matrix (block counts). */
+int monolis_b200_device_info(MONOLIS* mat, long long* nz_blocks, long long* padded_blocks, int* n_slices);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,110 @@
+// dev.h -- host-visible device data structures and kernel launchers.
+//
+// Device layout of one block-CSR matrix (N block rows of ndof x ndof blocks):
+// a sliced ELL ("SELL-32") copy built on the device from the uploaded CSR.
+// Rows are grouped in slices of 32 consecutive rows (one warp); slice s owns
+// 32 * w_s block slots, w_s = longest row in the slice. Slot k of the row at
+// lane l of slice s is block b = slptr[s] + 32*k + l; its column id is col[b]
+// and entry (r,c) of its value block is val[(slptr[s] + 32*k)*nd2 +
+// (r*ndof + c)*32 + l]. A warp therefore reads every value and column id as a
+// contiguous 128/256-byte line, one thread owns one block row and walks its
+// blocks in CSR (ascending column) order, which is the reference's summation
+// order. Padded slots (k >= row length) are never read: each thread stops at
+// its own row length, taken from the CSR offsets.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mb {
+
+// Status codes written to Iarray[MONOLIS_PRM_I_IERR] (see monolis_b200.h).
+enum Status : int {
+  kOk = 0,
+  kMaxIter = 1,
+  kBreakdown = 2,
+  kNonFinite = 3,
+  kTimeout = 4,
+  kBadInput = 5,
+  kCudaError = 6,
+  kZeroRhs = 7,  // internal: B2 == 0, x set to zero (reported as kOk)
+};
+
+struct SolverState {
+  double rho, rho1, alpha, beta, omega, c2, B2, resid, tol;
+  double rr, ts, tt;
+  // mixed precision (reliable updates)
+  double r_true0;     // ||b - A x0|| in FP64 (denominator of the relative residual)
+  double rmax;        // largest iterated-residual norm since the last FP64 refresh
+  double delta;       // refresh when ||r|| < delta * rmax
+  int iter, max_iter, done, status, iter_rr, n_refine, refresh, pad;
+};
+
+struct SellMatrix {
+  int N = 0, ndof = 0, nslices = 0;
+  long long nz = 0, padded = 0;
+  int* d_rowptr = nullptr;        // CSR offsets (N+1)
+  long long* d_slptr = nullptr;   // nslices+1, in blocks
+  int* d_col = nullptr;           // padded block column ids, 0-based
+  double* d_val64 = nullptr;
+  float* d_val32 = nullptr;
+  double* d_alu64 = nullptr;      // DIAG factors, entry-major: alu[e*N + row]
+  float* d_alu32 = nullptr;
+  // upload staging (kept between solves)
+  int* d_item = nullptr;          // CSR items as uploaded (1-based)
+  double* d_csrval = nullptr;
+  size_t cap_rowptr = 0, cap_slptr = 0, cap_col = 0, cap_val64 = 0, cap_val32 = 0;
+  size_t cap_alu64 = 0, cap_alu32 = 0, cap_item = 0, cap_csrval = 0;
+  bool have_val32 = false, have_alu = false, have_alu32 = false;
+};
+
+struct Scratch {
+  double* partials = nullptr;     // kMaxBlocks * 4 doubles
+  unsigned int* ticket = nullptr;
+  SolverState* st = nullptr;
+  SolverState* h_st = nullptr;    // pinned host mirror
+  double* hist = nullptr;         // residual history (max_iter + 1)
+  size_t hist_cap = 0;
+  size_t partials_cap = 0;
+};
+
+// ---- matrix build on the device ----
+int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const double* h_val,
+               int N, int ndof, cudaStream_t s, double* t_h2d);
+int sell_make_fp32(SellMatrix& m, cudaStream_t s);
+int diag_setup(SellMatrix& m, cudaStream_t s);  // FP64 (+FP32 copy when have_val32)
+void sell_free(SellMatrix& m);
+
+// ---- kernels callable on their own ----
+int spmv64(const SellMatrix& m, const double* x, double* y, cudaStream_t s);
+int spmv32(const SellMatrix& m, const float* x, float* y, cudaStream_t s);
+int dot64(long long n, const double* x, const double* y, double* out, Scratch& sc, cudaStream_t s);
+int diag_apply64(const SellMatrix& m, const double* x, double* y, cudaStream_t s);
+
+// ---- solvers (device-resident loops) ----
+struct SolveParams {
+  int method;        // MONOLIS_ITER_CG / MONOLIS_ITER_BICGSTAB
+  int precond;       // MONOLIS_PREC_NONE / MONOLIS_PREC_DIAG
+  int max_iter;
+  double tol;
+  int init_x;        // zero x before solving
+  int precision;     // 0 FP64, 1 FP32 inner + FP64 reliable refresh
+  double delta;      // refresh threshold for precision 1
+  int batch;         // iterations per graph launch
+  int use_graph;
+};
+struct SolveResult {
+  int iter = 0, status = 0, n_refine = 0;
+  double resid = 0.0;
+  double t_loop = 0.0;  // device loop seconds
+  long long launches = 0;  // kernels launched by the solve
+};
+
+int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double* d_b, double* d_x,
+                 SolveResult& res, double* h_hist, cudaStream_t s);
+
+int scratch_ensure(Scratch& sc, size_t hist_len);
+void scratch_free(Scratch& sc);
+
+}  // namespace mb

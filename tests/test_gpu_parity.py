@@ -1,0 +1,131 @@
+"""GPU parity: the CUDA path (libmonolis_b200.so) against the CPU oracle on
+the same seeded inputs, through the monolis C API.
+
+Tolerances: SpMV is bit-identical (same per-row summation order, no FMA
+contraction in the FP64 path); dot products differ only in summation order
+(relative 1e-13); FP64 CG/BiCGSTAB reproduce the oracle's iteration count
+within +-2 and its solution within 1e-10 relative (x is compared at the
+oracle's own tolerance, so the bound is on the difference of two converged
+iterates)."""
+import numpy as np
+import pytest
+
+from monolis_b200 import api
+from helpers import bits_equal, build, rel_err, solve
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("problem,kw", [
+    ("laplacian", dict(n=16)),
+    ("elasticity", dict(n=9)),
+    ("convection_diffusion", dict(n=12, peclet=5.0)),
+    ("diffusion_kappa", dict(n=9)),
+])
+def test_spmv_bit_exact(gpu, oracle, problem, kw):
+    mp, b = build(gpu, problem, **kw)
+    mo, _ = build(oracle, problem, **kw)
+    rng = np.random.default_rng(7)
+    for _ in range(3):
+        x = rng.standard_normal(len(b))
+        yo = mo.matvec(x)
+        yp = mp.matvec(x)
+        assert bits_equal(yp, yo)
+
+
+def test_spmv_ndof2_random_blocks(gpu, oracle):
+    # 10-node chain, ndof 2, like wrapper_test/solver/monolis_solver_c_test.c
+    elem = np.array([[i, i + 1] for i in range(9)], dtype=np.int32)
+    rng = np.random.default_rng(3)
+    vals = rng.standard_normal((9, 16))
+    out = []
+    for lib in (gpu, oracle):
+        m = api.Monolis(lib)
+        m.get_nonzero_pattern_by_simple_mesh(10, 2, 2, elem)
+        m.add_elements(elem, 2, vals.reshape(-1), 16)
+        x = np.linspace(-1, 1, 20)
+        out.append(m.matvec(x))
+    assert bits_equal(out[0], out[1])
+
+
+def test_inner_product(gpu, oracle):
+    mp, b = build(gpu, "laplacian", n=20)
+    mo, _ = build(oracle, "laplacian", n=20)
+    rng = np.random.default_rng(1)
+    x, y = rng.standard_normal(len(b)), rng.standard_normal(len(b))
+    sp = mp.inner_product(1, x, y)
+    so = mo.inner_product(1, x, y)
+    assert abs(sp - so) <= 1e-13 * np.abs(x * y).sum()
+
+
+@pytest.mark.parametrize("problem,kw,method", [
+    ("laplacian", dict(n=32), api.ITER_CG),          # the CPU-runnable configuration, full size
+    ("elasticity", dict(n=12), api.ITER_CG),
+    ("diffusion_kappa", dict(n=12), api.ITER_CG),
+    ("convection_diffusion", dict(n=24, peclet=0.5), api.ITER_BICGSTAB),
+    ("convection_diffusion", dict(n=24, peclet=5.0), api.ITER_BICGSTAB),
+    ("convection_diffusion", dict(n=24, peclet=50.0), api.ITER_BICGSTAB),
+    ("laplacian", dict(n=16), api.ITER_BICGSTAB),
+])
+@pytest.mark.parametrize("prec", [api.PREC_DIAG, api.PREC_NONE])
+def test_solver_parity_fp64(gpu, oracle, problem, kw, method, prec):
+    mp, b = build(gpu, problem, **kw)
+    mo, _ = build(oracle, problem, **kw)
+    xo, it_o, res_o, st_o = solve(mo, b, method, prec, tol=1e-8)
+    xp, it_p, res_p, st_p = solve(mp, b, method, prec, tol=1e-8)
+    assert st_o == 0 and st_p == 0, (st_o, st_p)
+    assert abs(it_p - it_o) <= 2, (it_p, it_o)
+    assert res_p < 1e-8
+    # both iterates satisfy the same tolerance; compare them at a tighter solve
+    xo2, _, _, _ = solve(mo, b, method, prec, tol=1e-12)
+    xp2, _, _, _ = solve(mp, b, method, prec, tol=1e-12)
+    assert rel_err(xp2, xo2) < 1e-10
+    assert rel_err(xp, xo) < 1e-6
+
+
+def test_cg_mixed_precision(gpu, oracle):
+    mp, b = build(gpu, "elasticity", n=12)
+    mo, _ = build(oracle, "elasticity", n=12)
+    xo, it_o, _, _ = solve(mo, b, api.ITER_CG, api.PREC_DIAG, tol=1e-12)
+    xm, it_m, res_m, st_m = solve(mp, b, api.ITER_CG, api.PREC_DIAG, tol=1e-8, precision=1)
+    assert st_m == 0 and res_m < 1e-8
+    # true FP64 residual of the mixed solution
+    r = b - mo.matvec(xm)
+    r0 = b
+    assert np.linalg.norm(r) / np.linalg.norm(r0) < 1.01e-8
+    assert mp.Iarray[api.B200_PRM_I_N_REFINE] >= 1
+    assert rel_err(xm, xo) < 1e-5
+
+
+def test_zero_rhs(gpu, oracle):
+    # src/linalg/mat_converge.f90:40-48: <r0,r0> == 0 -> X = 0, converged
+    for lib in (gpu, oracle):
+        m, b = build(lib, "laplacian", n=8)
+        x = np.ones_like(b)
+        m.set_init_x(True)
+        m.solve(np.zeros_like(b), x)
+        assert np.all(x == 0.0)
+        assert m.get_error_tag() == 0
+
+
+def test_maxiter_status(gpu, oracle):
+    mp, b = build(gpu, "laplacian", n=16)
+    _, it, _, st = solve(mp, b, maxiter=3)
+    assert st == 1 and it == 3
+
+
+def test_nonfinite_status(gpu):
+    mp, b = build(gpu, "laplacian", n=8)
+    b[5] = np.nan
+    _, _, _, st = solve(mp, b)
+    assert st == 3
+
+
+def test_warm_start(gpu, oracle):
+    mp, b = build(gpu, "laplacian", n=16)
+    mo, _ = build(oracle, "laplacian", n=16)
+    x0 = np.linspace(0, 1, len(b))
+    xo, it_o, _, _ = solve(mo, b, x0=x0)
+    xp, it_p, _, _ = solve(mp, b, x0=x0)
+    assert abs(it_o - it_p) <= 2
+    assert rel_err(xp, xo) < 1e-6
