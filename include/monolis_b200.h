@@ -33,6 +33,7 @@ static const int MONOLIS_B200_PRM_I_N_REFINE       = 33; /* out: FP64 residual r
 static const int MONOLIS_B200_PRM_I_BATCH          = 34; /* iterations per graph launch (0: 16) */
 static const int MONOLIS_B200_PRM_I_CHECK          = 35; /* 1: validate CSR index/item before upload */
 static const int MONOLIS_B200_PRM_I_LAUNCHES       = 36; /* out: kernels launched by the last solve */
+static const int MONOLIS_B200_PRM_I_ITER_RR        = 37; /* true-residual interval of CG/BiCGSTAB (0: 200, as the reference) */
 
 static const int MONOLIS_B200_PRM_R_REFINE_DELTA   = 30; /* refresh when ||r|| < delta*max||r|| (0: 0.1) */
 static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */

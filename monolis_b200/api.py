@@ -44,6 +44,8 @@ B200_PRM_I_MATRIX_VERSION = 32
 B200_PRM_I_N_REFINE = 33
 B200_PRM_I_BATCH = 34
 B200_PRM_I_CHECK = 35
+B200_PRM_I_LAUNCHES = 36
+B200_PRM_I_ITER_RR = 37
 B200_PRM_R_REFINE_DELTA = 30
 B200_PRM_R_TIME_H2D = 31
 B200_PRM_R_TIME_D2H = 32
@@ -152,6 +154,7 @@ _PRODUCT = {
 _ORACLE_EXTRA = {
     "oracle_set_threads": (None, [C.c_int]),
     "oracle_get_threads": (C.c_int, []),
+    "oracle_set_iter_rr": (None, [C.c_int]),
     "oracle_pattern_by_simple_mesh_flat": (None, [_MP, C.c_int, C.c_int, C.c_int, C.c_int, _ip]),
     "oracle_add_elements": (None, [_MP, C.c_int, C.c_int, _ip, _dp, C.c_longlong, _dp]),
     "oracle_diag_setup": (None, [_MP, _dp]),

@@ -400,6 +400,7 @@ int solve_resident(MONOLIS* m, DevState* s, const double* d_b, double* d_x, doub
   p.precision = I[MONOLIS_B200_PRM_I_PRECISION];
   p.delta = R[MONOLIS_B200_PRM_R_REFINE_DELTA];
   p.batch = I[MONOLIS_B200_PRM_I_BATCH];
+  p.iter_rr = I[MONOLIS_B200_PRM_I_ITER_RR];
   p.use_graph = 1;
   if (I[MONOLIS_PRM_I_SHOW_SUMMARY] == MONOLIS_I_TRUE)
     printf("** MONOLIS solver: %s, prec: %s\n", str_iter(p.method), str_prec(p.precond));

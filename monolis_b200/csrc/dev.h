@@ -38,7 +38,7 @@ struct SolverState {
   double r_true0;     // ||b - A x0|| in FP64 (denominator of the relative residual)
   double rmax;        // largest iterated-residual norm since the last FP64 refresh
   double delta;       // refresh when ||r|| < delta * rmax
-  int iter, max_iter, done, status, iter_rr, n_refine, refresh, pad;
+  int iter, max_iter, done, status, iter_rr, n_refine, refresh, rr_flag;  // rr_flag: true residual due this iteration
 };
 
 struct SellMatrix {
@@ -91,6 +91,7 @@ struct SolveParams {
   int init_x;        // zero x before solving
   int precision;     // 0 FP64, 1 FP32 inner + FP64 reliable refresh
   double delta;      // refresh threshold for precision 1
+  int iter_rr;       // true residual every iter_rr iterations (reference: 200)
   int batch;         // iterations per graph launch
   int use_graph;
 };

@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(kThreads)
                  T* __restrict__ z, T* __restrict__ rt, const T* __restrict__ alu, int prec, int mode, int gated,
                  double* partials, unsigned int* ticket, SolverState* st, double* hist) {
   if (st->done) return;
-  if (gated && (st->iter % st->iter_rr) != 0) return;
+  if (gated && !st->rr_flag) return;
   const bool init = st->iter == 0;
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
@@ -127,6 +127,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    st->rr_flag = 0;
     if (mode == 0) fin_cg(st, tot[0], tot[1], hist);
     else fin_bicg(st, tot[0], tot[1], hist);
   });
@@ -207,7 +208,12 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
-  if (rr_iter) return;
+  if (rr_iter) {
+    // iteration counter is not advanced here: the residual kernel that
+    // follows recomputes R = B - A X and finishes the iteration
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
+    return;
+  }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_cg(st, tot[0], tot[1], hist); });
 }
 
@@ -331,7 +337,10 @@ __global__ void __launch_bounds__(kThreads)
       v[1] += (double)rv * (double)rt[i];
     }
   }
-  if (rr_iter) return;
+  if (rr_iter) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
+    return;
+  }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_bicg(st, tot[0], tot[1], hist); });
 }
 
@@ -517,7 +526,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   SolverState h{};
   h.tol = p.tol;
   h.max_iter = p.max_iter;
-  h.iter_rr = 200;
+  h.iter_rr = p.iter_rr > 0 ? p.iter_rr : 200;
   h.delta = p.delta > 0 ? p.delta : 0.1;
   MB_CUDA_OK(cudaMemcpyAsync(sc.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
   MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * 64, s));

@@ -41,6 +41,10 @@
 
 namespace {
 
+// iter_RR of src/iterative/CG.f90:40 and BiCGSTAB.f90:41 (200); settable
+// through oracle_set_iter_rr() so tests can cross several replacements.
+int g_iter_rr = 200;
+
 double now_sec() {
   using namespace std::chrono;
   return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -388,7 +392,7 @@ bool check_converge(MONOLIS_PRM* prm, long long nndof, const double* R, double B
 int solver_CG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
   double* X = a->R.X;
   const double* B = a->R.B;
-  const int iter_RR = 200;
+  const int iter_RR = g_iter_rr;
   long long nndof = (long long)a->N * a->NDOF;
   if (prm->Iarray[MONOLIS_PRM_I_IS_INIT_X] == MONOLIS_I_TRUE)
     for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
@@ -436,7 +440,7 @@ int solver_CG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
 int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
   double* X = a->R.X;
   const double* B = a->R.B;
-  const int iter_RR = 200;
+  const int iter_RR = g_iter_rr;
   long long nndof = (long long)a->N * a->NDOF;
   if (prm->Iarray[MONOLIS_PRM_I_IS_INIT_X] == MONOLIS_I_TRUE)
     for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
@@ -826,6 +830,8 @@ void oracle_set_threads(int n) {
   (void)n;
 #endif
 }
+void oracle_set_iter_rr(int n) { g_iter_rr = n > 0 ? n : 200; }
+
 int oracle_get_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -83,6 +83,59 @@ def test_solver_parity_fp64(gpu, oracle, problem, kw, method, prec):
     assert rel_err(xp, xo) < 1e-6
 
 
+def test_cg_parity_past_residual_replacement(gpu, oracle):
+    # 277 oracle iterations: crosses the true-residual replacement at 200
+    mp, b = build(gpu, "elasticity", n=24)
+    mo, _ = build(oracle, "elasticity", n=24)
+    xo, it_o, _, st_o = solve(mo, b, api.ITER_CG, api.PREC_DIAG)
+    xp, it_p, _, st_p = solve(mp, b, api.ITER_CG, api.PREC_DIAG)
+    assert it_o > 200 and st_o == 0 and st_p == 0
+    assert abs(it_p - it_o) <= 2, (it_p, it_o)
+    assert rel_err(xp, xo) < 1e-6
+
+
+@pytest.mark.parametrize("problem,kw,method,prec,rr", [
+    ("convection_diffusion", dict(n=48, peclet=5.0), api.ITER_BICGSTAB, api.PREC_DIAG, 20),
+    ("convection_diffusion", dict(n=32, peclet=0.5), api.ITER_BICGSTAB, api.PREC_DIAG, 10),
+    ("convection_diffusion", dict(n=40, peclet=50.0), api.ITER_BICGSTAB, api.PREC_DIAG, 15),
+    ("diffusion_kappa", dict(n=24), api.ITER_CG, api.PREC_DIAG, 25),
+    ("elasticity", dict(n=16), api.ITER_CG, api.PREC_NONE, 30),
+])
+def test_parity_with_frequent_residual_replacement(gpu, oracle, problem, kw, method, prec, rr):
+    """The replacement interval (200 in the reference) shortened in both
+    libraries, so a well-conditioned solve crosses it several times."""
+    mp, b = build(gpu, problem, **kw)
+    mo, _ = build(oracle, problem, **kw)
+    mp.Iarray[api.B200_PRM_I_ITER_RR] = rr
+    oracle.oracle_set_iter_rr(rr)
+    try:
+        xo, it_o, _, st_o = solve(mo, b, method, prec)
+    finally:
+        oracle.oracle_set_iter_rr(200)
+    xp, it_p, _, st_p = solve(mp, b, method, prec)
+    assert it_o > 2 * rr and st_o == 0 and st_p == 0
+    assert abs(it_p - it_o) <= 2, (it_p, it_o)
+    assert rel_err(xp, xo) < 1e-6
+
+
+@pytest.mark.parametrize("problem,kw,method,prec,tol", [
+    ("diffusion_kappa", dict(n=32), api.ITER_BICGSTAB, api.PREC_NONE, 1e-12),
+    ("elasticity", dict(n=20), api.ITER_BICGSTAB, api.PREC_NONE, 1e-10),
+])
+def test_bicgstab_chaotic_cases_converge(gpu, oracle, problem, kw, method, prec, tol):
+    """Unpreconditioned BiCGSTAB driven to 1e-10..1e-12: the iteration count
+    depends on summation order (the oracle alone gives 348..381 and 235..240
+    across 1..8 OpenMP threads), so only convergence and the solution are
+    compared."""
+    mp, b = build(gpu, problem, **kw)
+    mo, _ = build(oracle, problem, **kw)
+    xo, it_o, _, st_o = solve(mo, b, method, prec, tol=tol)
+    xp, it_p, res_p, st_p = solve(mp, b, method, prec, tol=tol)
+    assert st_o == 0 and st_p == 0 and res_p < tol
+    assert abs(it_p - it_o) <= 0.15 * it_o, (it_p, it_o)
+    assert rel_err(xp, xo) < 1e-6
+
+
 def test_cg_mixed_precision(gpu, oracle):
     mp, b = build(gpu, "elasticity", n=12)
     mo, _ = build(oracle, "elasticity", n=12)
@@ -129,3 +182,20 @@ def test_warm_start(gpu, oracle):
     xp, it_p, _, _ = solve(mp, b, x0=x0)
     assert abs(it_o - it_p) <= 2
     assert rel_err(xp, xo) < 1e-6
+
+
+def test_fullsize_elasticity_fp64_iterations(gpu):
+    """128^3-node elasticity (55.7 M blocks): the FP64 GPU CG against the
+    oracle's iteration count for the same system (tests/golden/
+    oracle_iterations.json, written by oracle/iterations.py with serial sums)."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "oracle_iterations.json")) as f:
+        it_oracle = json.load(f)["elasticity_n128_cg_diag_tol1e-08"]
+    mp, b = build(gpu, "elasticity", n=128)
+    x, it, res, st = solve(mp, b, api.ITER_CG, api.PREC_DIAG)
+    assert st == 0 and res < 1e-8
+    assert abs(it - it_oracle) <= 2, (it, it_oracle)
+    # size-independent check: the FP64 device SpMV of the solution reproduces b
+    r = b - mp.matvec(x)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-8
