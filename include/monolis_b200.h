@@ -91,6 +91,23 @@ int monolis_b200_device_matvec_R32(MONOLIS* mat, const float* d_x, float* d_y);
 /* Layout facts of the prepared device matrix (block counts). */
 int monolis_b200_device_info(MONOLIS* mat, long long* nz_blocks, long long* padded_blocks, int* n_slices);
 
+/* ---- allocation-free inner product ----
+ * No counterpart in the reference library.
+ * *d_sum = sum_i d_x[i]*d_y[i] for device vectors of length n, enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream), FP64 accumulation.
+ * For callers that cannot call cudaMalloc when they need the result (an
+ * application that reserved all device memory for its own pool, a loop that
+ * must not take cudaMalloc's implicit synchronisation): this entry point
+ * never allocates. Its reduction scratch is a fixed array in the library's
+ * device image, held by every GPU that loads the library until the process
+ * exits, which caps n at 16,777,216 elements; larger n is rejected with
+ * MONOLIS_B200_BAD_INPUT and an error message. The first call on each device
+ * looks up that array's address (make it before any stream capture). All
+ * calls share the one array: calls that overlap on the GPU (different
+ * streams, or other host threads) race and must be serialised by the caller. */
+int monolis_b200_inner_product_noalloc_R(long long n, const double* d_x, const double* d_y, double* d_sum,
+                                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -149,6 +149,8 @@ _PRODUCT = {
     "monolis_b200_device_matvec_R32": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
     "monolis_b200_device_info": (C.c_int, [_MP, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                            C.POINTER(C.c_int)]),
+    "monolis_b200_inner_product_noalloc_R": (C.c_int, [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                       C.c_void_p]),
 }
 
 _ORACLE_EXTRA = {
