@@ -6,6 +6,11 @@ extrapolation count of the CPU baseline).
 
 Runs the CPU oracle (oracle/_build/libmonolis_oracle.so); long at full size
 (minutes per system on a few cores). Keys: <problem>_n<size>[_pe<P>]_<method>_<prec>_tol<tol>.
+
+--spread runs each case with 2, 4 and 8 OpenMP threads instead (three more
+summation orders of every dot product) and stores the counts under
+"<key>:by_threads": how far the iteration count moves when only the
+summation order changes.
 """
 import argparse
 import json
@@ -40,6 +45,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--only", nargs="*")
+    ap.add_argument("--spread", action="store_true")
     args = ap.parse_args()
     lib = api.load_library(SO, oracle=True)
     lib.oracle_set_threads(args.threads)
@@ -49,6 +55,29 @@ def main():
             data = json.load(f)
     for key, (fn, kw, method, tol) in CASES.items():
         if args.only and key not in args.only:
+            continue
+        if args.spread:
+            counts = {}
+            for th in (2, 4, 8):
+                lib.oracle_set_threads(th)
+                m = api.Monolis(lib)
+                b = fn(m, **kw)
+                if isinstance(b, tuple):
+                    b = b[0]
+                m.quiet()
+                m.set_error_abort(False)
+                m.set_method(method)
+                m.set_precond(api.PREC_DIAG)
+                m.set_tolerance(tol)
+                m.set_maxiter(100000)
+                x = np.zeros_like(b)
+                m.solve(b, x)
+                counts[str(th)] = m.get_converge_iter()
+                m.finalize()
+                print(key, th, counts[str(th)], flush=True)
+            data[key + ":by_threads"] = counts
+            with open(OUT, "w") as f:
+                json.dump(data, f, indent=1, sort_keys=True)
             continue
         m = api.Monolis(lib)
         b = fn(m, **kw)
