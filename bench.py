@@ -242,12 +242,14 @@ def main():
     times, iters = [], []
     launches = 0
     barrier()
+    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx-include "timed/" selects these launches
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t, it, res = timed_solve(1)
             times.append(t)
             iters.append(it)
-            launches += int(m.Iarray[36])
+            launches += int(m.Iarray[api.B200_PRM_I_LAUNCHES])
+    torch.cuda.nvtx.range_pop()
     barrier()
     clocks = clk.summary()
     t_mixed = float(np.mean(times))
@@ -262,6 +264,7 @@ def main():
 
     # SpMV roofline (standalone kernels, FP64 and FP32), CUDA events on the library stream
     nzb, padded, nslices = m.device_info()
+    u64, u32 = int(m.Iarray[api.B200_PRM_I_UNROLL_FP64]), int(m.Iarray[api.B200_PRM_I_UNROLL_FP32])
     xs64 = torch.randn(n_unk, dtype=torch.float64, device="cuda")
     ys64 = torch.empty_like(xs64)
     xs32 = xs64.float()
@@ -365,6 +368,7 @@ def main():
             "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call"},
             "gpu_launches": launches,
+            "autotuned_unroll": {"fp64": u64, "fp32": u32},
             "clocks": clocks,
             "cpu_baseline": cpu,
             "assembly_s": t_asm,

@@ -34,11 +34,21 @@ static const int MONOLIS_B200_PRM_I_BATCH          = 34; /* iterations per graph
 static const int MONOLIS_B200_PRM_I_CHECK          = 35; /* 1: validate CSR index/item before upload */
 static const int MONOLIS_B200_PRM_I_LAUNCHES       = 36; /* out: kernels launched by the last solve */
 static const int MONOLIS_B200_PRM_I_ITER_RR        = 37; /* true-residual interval of CG/BiCGSTAB (0: 200, as the reference) */
+static const int MONOLIS_B200_PRM_I_UNROLL_FP64    = 38; /* out: SpMV unroll depth picked by the autotuner (FP64) */
+static const int MONOLIS_B200_PRM_I_UNROLL_FP32    = 39; /* out: same for the FP32 layout */
+static const int MONOLIS_B200_PRM_I_KERNEL_TIMERS  = 40; /* 1: time every kernel with CUDA events (no graph; slower loop);
+                                                            fills TIME_SPMV / DOTP / PREC and TIME_KERNEL+k */
+static const int MONOLIS_B200_PRM_I_REFRESH_PERIOD = 41; /* mixed precision: FP64 residual refresh at the latest
+                                                            n iterations after the previous one (0: no limit) */
 
-static const int MONOLIS_B200_PRM_R_REFINE_DELTA   = 30; /* refresh when ||r|| < delta*max||r|| (0: 0.1) */
+static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
+                                                            below delta * its largest value since the last one
+                                                            (0: 0.1) */
 static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */
 static const int MONOLIS_B200_PRM_R_TIME_D2H       = 32; /* out: seconds spent on device->host copies */
 static const int MONOLIS_B200_PRM_R_TIME_LOOP      = 33; /* out: seconds in the device iteration loop */
+static const int MONOLIS_B200_PRM_R_TIME_KERNEL    = 40; /* out, timing mode: seconds per kernel slot k of an
+                                                            iteration in Rarray[40 + k], k < 8 */
 
 static const int MONOLIS_B200_PRECISION_FP64  = 0;
 static const int MONOLIS_B200_PRECISION_MIXED = 1;

@@ -371,6 +371,8 @@ int prepare(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32, double* t_h
     int rc = mb::sell_make_fp32(s->A, st);
     if (rc) return rc;
   }
+  m->prm.Iarray[MONOLIS_B200_PRM_I_UNROLL_FP64] = s->A.u64;
+  m->prm.Iarray[MONOLIS_B200_PRM_I_UNROLL_FP32] = s->A.have_val32 ? s->A.u32 : 0;
   return mb::kOk;
 }
 
@@ -398,9 +400,11 @@ int solve_resident(MONOLIS* m, DevState* s, const double* d_b, double* d_x, doub
   p.tol = R[MONOLIS_PRM_R_TOL];
   p.init_x = I[MONOLIS_PRM_I_IS_INIT_X] == MONOLIS_I_TRUE;
   p.precision = I[MONOLIS_B200_PRM_I_PRECISION];
-  p.delta = R[MONOLIS_B200_PRM_R_REFINE_DELTA];
+  p.delta = R[MONOLIS_B200_PRM_R_REFRESH_DELTA];
+  p.refresh_period = I[MONOLIS_B200_PRM_I_REFRESH_PERIOD];
   p.batch = I[MONOLIS_B200_PRM_I_BATCH];
   p.iter_rr = I[MONOLIS_B200_PRM_I_ITER_RR];
+  p.timers = I[MONOLIS_B200_PRM_I_KERNEL_TIMERS] == 1;
   p.use_graph = 1;
   if (I[MONOLIS_PRM_I_SHOW_SUMMARY] == MONOLIS_I_TRUE)
     printf("** MONOLIS solver: %s, prec: %s\n", str_iter(p.method), str_prec(p.precond));
@@ -425,7 +429,14 @@ int solve_resident(MONOLIS* m, DevState* s, const double* d_b, double* d_x, doub
   R[MONOLIS_R_TIME_PREP] = t_prep;
   R[MONOLIS_B200_PRM_R_TIME_H2D] = t_h2d;
   R[MONOLIS_B200_PRM_R_TIME_LOOP] = res.t_loop;
-  R[MONOLIS_R_TIME_SPMV] = R[MONOLIS_R_TIME_DOTP] = R[MONOLIS_R_TIME_PREC] = 0.0;
+  // fused kernels: SpMV time = SpMV kernels (with their fused dots), precond
+  // time = update kernels that apply M^-1 (with their AXPYs and dots), inner
+  // product time = the remaining vector kernels; filled in timing mode only
+  R[MONOLIS_R_TIME_SPMV] = res.t_kind[0];
+  R[MONOLIS_R_TIME_DOTP] = res.t_kind[1];
+  R[MONOLIS_R_TIME_PREC] = res.t_kind[2];
+  for (int k = 0; k < 8; k++)
+    R[MONOLIS_B200_PRM_R_TIME_KERNEL + k] = k < (int)res.kernel_time.size() ? res.kernel_time[k] : 0.0;
   R[MONOLIS_R_TIME_COMM_DOTP] = R[MONOLIS_R_TIME_COMM_SPMV] = 0.0;
   R[MONOLIS_R_TIME_SOL] = now_sec() - t_start;
   return mb::kOk;

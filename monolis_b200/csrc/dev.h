@@ -17,6 +17,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 namespace mb {
 
 // Status codes written to Iarray[MONOLIS_PRM_I_IERR] (see monolis_b200.h).
@@ -34,11 +36,16 @@ enum Status : int {
 struct SolverState {
   double rho, rho1, alpha, beta, omega, c2, B2, resid, tol;
   double rr, ts, tt;
-  // mixed precision (reliable updates)
-  double r_true0;     // ||b - A x0|| in FP64 (denominator of the relative residual)
-  double rmax;        // largest iterated-residual norm since the last FP64 refresh
-  double delta;       // refresh when ||r|| < delta * rmax
-  int iter, max_iter, done, status, iter_rr, n_refine, refresh, rr_flag;  // rr_flag: true residual due this iteration
+  double rmax;   // mixed: largest iterated-residual norm since the last refresh
+  double delta;  // mixed: refresh when the residual norm < delta * rmax
+  int iter, max_iter, done, status;
+  int iter_rr;   // true residual every iter_rr iterations (FP64 CG / BiCGSTAB)
+  int rr_flag;   // true residual due in this iteration
+  int period;    // mixed: refresh at the latest `period` iterations after the last (0: no limit)
+  int last_refresh;
+  int refresh;   // mixed: refresh due in this iteration
+  int fold;      // mixed: y still to be folded into x
+  int n_refine;  // mixed: refreshes done
 };
 
 struct SellMatrix {
@@ -48,14 +55,23 @@ struct SellMatrix {
   long long* d_slptr = nullptr;   // nslices+1, in blocks
   int* d_col = nullptr;           // padded block column ids, 0-based
   double* d_val64 = nullptr;
-  float* d_val32 = nullptr;
+  float* d_val32 = nullptr;       // FP32 values in the paired layout below
+  // FP32 copy in the paired layout: slices of 64 rows, lane l of a warp owns
+  // rows 64s+2l and 64s+2l+1, so values and column ids are read as float2 /
+  // int2 (8 bytes per lane, the byte rate of the FP64 layout).
+  int nslices2 = 0;
+  long long padded2 = 0;
+  long long* d_slptr2 = nullptr;  // nslices2+1, in blocks
+  int* d_col2 = nullptr;
+  // unroll depth (slots in flight per thread) picked by the autotuner
+  int u64 = 2, u32 = 2;
   double* d_alu64 = nullptr;      // DIAG factors, entry-major: alu[e*N + row]
   float* d_alu32 = nullptr;
   // upload staging (kept between solves)
   int* d_item = nullptr;          // CSR items as uploaded (1-based)
   double* d_csrval = nullptr;
   size_t cap_rowptr = 0, cap_slptr = 0, cap_col = 0, cap_val64 = 0, cap_val32 = 0;
-  size_t cap_alu64 = 0, cap_alu32 = 0, cap_item = 0, cap_csrval = 0;
+  size_t cap_alu64 = 0, cap_alu32 = 0, cap_item = 0, cap_csrval = 0, cap_slptr2 = 0, cap_col2 = 0;
   bool have_val32 = false, have_alu = false, have_alu32 = false;
 };
 
@@ -73,6 +89,8 @@ struct Scratch {
 int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const double* h_val,
                int N, int ndof, cudaStream_t s, double* t_h2d);
 int sell_make_fp32(SellMatrix& m, cudaStream_t s);
+// Times the SpMV unroll variants on the matrix and keeps the fastest (u64 / u32).
+int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s);
 int diag_setup(SellMatrix& m, cudaStream_t s);  // FP64 (+FP32 copy when have_val32)
 void sell_free(SellMatrix& m);
 
@@ -90,16 +108,20 @@ struct SolveParams {
   double tol;
   int init_x;        // zero x before solving
   int precision;     // 0 FP64, 1 FP32 inner + FP64 reliable refresh
-  double delta;      // refresh threshold for precision 1
+  double delta;        // precision 1: refresh when ||r|| < delta * max ||r|| since the last one (0: 0.1)
+  int refresh_period;  // precision 1: refresh at the latest every n iterations (0: no limit)
   int iter_rr;       // true residual every iter_rr iterations (reference: 200)
   int batch;         // iterations per graph launch
   int use_graph;
+  int timers;        // time every kernel with CUDA events (no graph)
 };
 struct SolveResult {
   int iter = 0, status = 0, n_refine = 0;
   double resid = 0.0;
   double t_loop = 0.0;  // device loop seconds
   long long launches = 0;  // kernels launched by the solve
+  std::vector<double> kernel_time;     // timers: seconds per kernel slot of an iteration
+  double t_kind[3] = {0.0, 0.0, 0.0};  // timers: SpMV / other vector / precond kernels
 };
 
 int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double* d_b, double* d_x,

@@ -26,15 +26,50 @@ cudaError_t grow(P** p, size_t& cap, size_t need) {
   return e;
 }
 
-__global__ void slice_width_kernel(const int* __restrict__ rowptr, int N, int nslices, long long* __restrict__ width) {
+// Slots of slice s (h rows): h times the longest row of the slice.
+__global__ void slice_width_kernel(const int* __restrict__ rowptr, int N, int nslices, int h,
+                                   long long* __restrict__ width) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nslices) return;
   int w = 0;
-  for (int l = 0; l < kSlice; l++) {
-    int r = s * kSlice + l;
+  for (int l = 0; l < h; l++) {
+    int r = s * h + l;
     if (r < N) w = max(w, rowptr[r + 1] - rowptr[r]);
   }
-  width[s] = (long long)w * kSlice;
+  width[s] = (long long)w * h;
+}
+
+// Paired FP32 layout: one warp per slice of 64 rows, lane l writes rows
+// 64s+2l and 64s+2l+1 at adjacent positions of every slot line.
+template <int B>
+__global__ void sell2_fill_kernel(const int* __restrict__ rowptr, const int* __restrict__ item,
+                                  const double* __restrict__ csrval, const long long* __restrict__ slptr2, int N,
+                                  int nslices, int* __restrict__ col, float* __restrict__ val) {
+  constexpr int B2 = B * B;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nslices) return;
+  const long long base = slptr2[warp];
+  const int w = (int)((slptr2[warp + 1] - base) / 64);
+#pragma unroll
+  for (int j = 0; j < 2; j++) {
+    const int row = warp * 64 + 2 * lane + j;
+    const int len = row < N ? rowptr[row + 1] - rowptr[row] : 0;
+    const long long j0 = row < N ? rowptr[row] : 0;
+    for (int k = 0; k < w; k++) {
+      const long long slot = base + (long long)k * 64;
+      const long long pos = 2 * lane + j;
+      if (k < len) {
+        col[slot + pos] = item[j0 + k] - 1;
+#pragma unroll
+        for (int e = 0; e < B2; e++) val[slot * B2 + (long long)e * 64 + pos] = (float)csrval[(j0 + k) * B2 + e];
+      } else {
+        col[slot + pos] = row < N ? row : 0;
+#pragma unroll
+        for (int e = 0; e < B2; e++) val[slot * B2 + (long long)e * 64 + pos] = 0.0f;
+      }
+    }
+  }
 }
 
 // One warp per slice: lane l copies row (32s + l) into the slot-major layout.
@@ -121,6 +156,20 @@ __global__ void __launch_bounds__(256) spmv_kernel(SellView<V> A, const T* __res
   for (int r = 0; r < B; r++) y[(long long)row * B + r] = acc[r];
 }
 
+template <int B, int U>
+__global__ void __launch_bounds__(256) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (2 * t >= A.N) return;
+  float y0[B], y1[B];
+  sell_row2<B, U>(A, x, t, y0, y1);
+#pragma unroll
+  for (int r = 0; r < B; r++) y[(long long)2 * t * B + r] = y0[r];
+  if (2 * t + 1 < A.N) {
+#pragma unroll
+    for (int r = 0; r < B; r++) y[(long long)(2 * t + 1) * B + r] = y1[r];
+  }
+}
+
 template <class T>
 __global__ void dot_kernel(long long n, const T* __restrict__ x, const T* __restrict__ y, double* partials,
                            unsigned int* ticket, double* out) {
@@ -188,7 +237,7 @@ int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const doubl
   // slice widths -> prefix on the host (nslices = N/32 values) -> slice pointers
   long long* d_w = nullptr;
   MB_CUDA_OK(cudaMallocAsync((void**)&d_w, sizeof(long long) * nslices, s));
-  slice_width_kernel<<<(nslices + 255) / 256, 256, 0, s>>>(m.d_rowptr, N, nslices, d_w);
+  slice_width_kernel<<<(nslices + 255) / 256, 256, 0, s>>>(m.d_rowptr, N, nslices, kSlice, d_w);
   std::vector<long long> w(nslices), ptr(nslices + 1);
   MB_CUDA_OK(cudaMemcpyAsync(w.data(), d_w, sizeof(long long) * nslices, cudaMemcpyDeviceToHost, s));
   MB_CUDA_OK(cudaStreamSynchronize(s));
@@ -216,14 +265,35 @@ int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const doubl
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
-  return kOk;
+  return sell_autotune(m, false, s);
 }
 
 int sell_make_fp32(SellMatrix& m, cudaStream_t s) {
   if (m.have_val32) return kOk;
-  const long long n = m.padded * m.ndof * m.ndof;
-  MB_CUDA_OK(grow(&m.d_val32, m.cap_val32, (size_t)n));
-  to_fp32_kernel<<<148 * 8, 256, 0, s>>>(m.d_val64, m.d_val32, n);
+  const int N = m.N, B2 = m.ndof * m.ndof;
+  const int ns = (N + 63) / 64;
+  long long* d_w = nullptr;
+  MB_CUDA_OK(cudaMallocAsync((void**)&d_w, sizeof(long long) * ns, s));
+  slice_width_kernel<<<(ns + 255) / 256, 256, 0, s>>>(m.d_rowptr, N, ns, 64, d_w);
+  std::vector<long long> w(ns), ptr(ns + 1);
+  MB_CUDA_OK(cudaMemcpyAsync(w.data(), d_w, sizeof(long long) * ns, cudaMemcpyDeviceToHost, s));
+  MB_CUDA_OK(cudaStreamSynchronize(s));
+  cudaFreeAsync(d_w, s);
+  ptr[0] = 0;
+  for (int i = 0; i < ns; i++) ptr[i + 1] = ptr[i] + w[i];
+  m.nslices2 = ns;
+  m.padded2 = ptr[ns];
+  MB_CUDA_OK(grow(&m.d_slptr2, m.cap_slptr2, (size_t)ns + 1));
+  MB_CUDA_OK(grow(&m.d_col2, m.cap_col2, (size_t)m.padded2));
+  MB_CUDA_OK(grow(&m.d_val32, m.cap_val32, (size_t)m.padded2 * B2));
+  MB_CUDA_OK(cudaMemcpyAsync(m.d_slptr2, ptr.data(), sizeof(long long) * (ns + 1), cudaMemcpyHostToDevice, s));
+  int rc = dispatch_ndof(m.ndof, [&](auto Bc) {
+    constexpr int B = decltype(Bc)::value;
+    sell2_fill_kernel<B><<<(ns * 32 + 255) / 256, 256, 0, s>>>(m.d_rowptr, m.d_item, m.d_csrval, m.d_slptr2, N, ns,
+                                                              m.d_col2, m.d_val32);
+    return kOk;
+  });
+  if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
   m.have_val32 = true;
   if (m.have_alu) {
@@ -233,7 +303,7 @@ int sell_make_fp32(SellMatrix& m, cudaStream_t s) {
     MB_CUDA_OK(cudaGetLastError());
     m.have_alu32 = true;
   }
-  return kOk;
+  return sell_autotune(m, true, s);
 }
 
 int diag_setup(SellMatrix& m, cudaStream_t s) {
@@ -267,33 +337,101 @@ void sell_free(SellMatrix& m) {
   cudaFree(m.d_alu32);
   cudaFree(m.d_item);
   cudaFree(m.d_csrval);
+  cudaFree(m.d_slptr2);
+  cudaFree(m.d_col2);
   m = SellMatrix();
 }
 
-int spmv64(const SellMatrix& m, const double* x, double* y, cudaStream_t s) {
+template <class F>
+int dispatch_u(int u, F&& f) {
+  switch (u) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    default: return f(std::integral_constant<int, 2>{});
+  }
+}
+
+int spmv64_u(const SellMatrix& m, int u, const double* x, double* y, cudaStream_t s) {
   SellView<double> A = view_of<double>(m);
   int rc = dispatch_ndof(m.ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
-    constexpr int U = B == 1 ? 4 : (B <= 3 ? 2 : 1);
-    spmv_kernel<B, U, double, double><<<(m.N + 255) / 256, 256, 0, s>>>(A, x, y);
-    return kOk;
+    return dispatch_u(u, [&](auto Uc) {
+      constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
+      spmv_kernel<B, U, double, double><<<(m.N + 255) / 256, 256, 0, s>>>(A, x, y);
+      return (int)kOk;
+    });
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
   return kOk;
 }
 
-int spmv32(const SellMatrix& m, const float* x, float* y, cudaStream_t s) {
+int spmv32_u(const SellMatrix& m, int u, const float* x, float* y, cudaStream_t s) {
   if (!m.have_val32) return kBadInput;
-  SellView<float> A = view_of<float>(m);
+  SellView2 A = view2_of(m);
+  const int threads = (m.N + 1) / 2;
   int rc = dispatch_ndof(m.ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
-    constexpr int U = B == 1 ? 4 : (B <= 3 ? 2 : 1);
-    spmv_kernel<B, U, float, float><<<(m.N + 255) / 256, 256, 0, s>>>(A, x, y);
-    return kOk;
+    return dispatch_u(u, [&](auto Uc) {
+      constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
+      spmv2_kernel<B, U><<<(threads + 255) / 256, 256, 0, s>>>(A, x, y);
+      return (int)kOk;
+    });
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
+  return kOk;
+}
+
+int spmv64(const SellMatrix& m, const double* x, double* y, cudaStream_t s) { return spmv64_u(m, m.u64, x, y, s); }
+int spmv32(const SellMatrix& m, const float* x, float* y, cudaStream_t s) { return spmv32_u(m, m.u32, x, y, s); }
+
+// Unroll depth per matrix: each variant is launched 3 times on zero vectors
+// (the kernels have no data-dependent control flow) and the fastest kept.
+int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s) {
+  if (m.ndof >= 4) {
+    m.u64 = m.u32 = 1;
+    return kOk;
+  }
+  const size_t n = (size_t)m.N * m.ndof;
+  const size_t bytes = n * (fp32 ? sizeof(float) : sizeof(double));
+  void *x = nullptr, *y = nullptr;
+  MB_CUDA_OK(cudaMallocAsync(&x, bytes + 16, s));
+  MB_CUDA_OK(cudaMallocAsync(&y, bytes + 16, s));
+  MB_CUDA_OK(cudaMemsetAsync(x, 0, bytes, s));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_u = 2;
+  int rc = kOk;
+  for (int u = 1; u <= 3 && rc == kOk; u++) {
+    auto run = [&]() {
+      return fp32 ? spmv32_u(m, u, (const float*)x, (float*)y, s) : spmv64_u(m, u, (const double*)x, (double*)y, s);
+    };
+    rc = run();  // warm
+    if (rc) break;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; r++) run();
+    cudaEventRecord(e1, s);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = kCudaError;
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) {
+      best = ms;
+      best_u = u;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(x, s);
+  cudaFreeAsync(y, s);
+  if (rc) return rc;
+  if (fp32) m.u32 = best_u;
+  else m.u64 = best_u;
   return kOk;
 }
 

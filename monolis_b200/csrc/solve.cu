@@ -1,13 +1,22 @@
 // solve.cu -- device-resident CG and BiCGSTAB (FP64, and FP32-inner with
-// FP64 reliable-update refinement) built from fused kernels.
+// FP64 refinement) built from fused kernels.
 //
 // Every scalar of the recurrences (rho, alpha, beta, omega, B2, the
 // residual) lives in SolverState on the device. Each reduction is a one-pass
 // grid reduction whose last block also evaluates the scalar update, so an
-// iteration is a fixed sequence of kernels with no host round trip. The host
-// captures `batch` iterations into one CUDA graph, launches it repeatedly
-// and reads the done flag once per launch (two launches in flight); kernels
-// return immediately once `done` is set.
+// iteration is a fixed sequence of kernels with no host round trip. Kernels
+// that reduce run on a persistent grid (as many blocks as fit on the GPU at
+// once), so the arrival ticket sees one atomic per resident block.
+//
+// The host captures `batch` iterations into a CUDA graph and launches it
+// repeatedly, reading the state word once per launch with two launches in
+// flight; kernels return immediately once `done` is set. The true residual
+// every iter_RR iterations of FP64 CG/BiCGSTAB falls on the last iteration of
+// a batch (the batch divides iter_RR) and uses a second graph that contains
+// the residual kernel, so no other iteration pays for it. The FP64 refresh of
+// the mixed solver is decided on the device from the residual history; its
+// kernel sits in every iteration on a small grid and returns at once when
+// there is nothing to do.
 //
 // FP64 CG follows src/iterative/CG.f90:74-101 and BiCGSTAB follows
 // src/iterative/BiCGSTAB.f90:87-170 operation by operation (same vector
@@ -18,6 +27,8 @@
 #include <cmath>
 #include <cstdio>
 #include <functional>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "spmv.cuh"
@@ -26,9 +37,35 @@ namespace mb {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kVecBlocks = 148 * 8;
 
 inline int blocks_for(long long n) { return (int)((n + kThreads - 1) / kThreads); }
+
+int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int d = 0;
+    cudaGetDevice(&d);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, d);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+// Persistent grid of a kernel: resident blocks per SM x SMs.
+template <class K>
+int pgrid(K kernel) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  const void* key = reinterpret_cast<const void*>(kernel);
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kThreads, 0) != cudaSuccess || b < 1) b = 1;
+  const int g = b * num_sms();
+  cache[key] = g;
+  return g;
+}
 
 // ---------------------------------------------------------------------------
 // Scalar updates run by the last block of a grid reduction.
@@ -81,21 +118,21 @@ __device__ void fin_bicg(SolverState* st, double rr, double rrt, double* hist) {
 }
 
 // ---------------------------------------------------------------------------
-// Residual kernel: r = b - A x, then z = M^-1 r (CG) and the two dots.
+// FP64 residual kernel: r = b - A x, then z = M^-1 r (CG) and the two dots.
 // mode 0: CG (dots <r,r>, <r,z>); mode 1: BiCGSTAB (dots <r,r>, <r,rt>;
-// at iter 0 also rt = r). gated: run only on iterations with iter % 200 == 0.
+// at iter 0 also rt = r). Runs for the initial residual and, on iterations
+// with iter % iter_RR == 0, after the update kernel has raised rr_flag.
 // ---------------------------------------------------------------------------
 template <int B, int U, class V, class T>
 __global__ void __launch_bounds__(kThreads)
     resid_kernel(SellView<V> A, const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ r,
-                 T* __restrict__ z, T* __restrict__ rt, const T* __restrict__ alu, int prec, int mode, int gated,
+                 T* __restrict__ z, T* __restrict__ rt, const T* __restrict__ alu, int prec, int mode,
                  double* partials, unsigned int* ticket, SolverState* st, double* hist) {
   if (st->done) return;
-  if (gated && !st->rr_flag) return;
   const bool init = st->iter == 0;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!init && !st->rr_flag) return;
   double v[2] = {0.0, 0.0};
-  if (row < A.N) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T y[B];
     sell_row<B, U, V, T>(A, x, row, y);
     T t[B];
@@ -136,13 +173,42 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // CG kernels
 // ---------------------------------------------------------------------------
+template <class T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec16<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
 // P = beta*P + 1.0*Z (src/iterative/CG.f90:78-83); P = Z on iteration 1.
+// 16-byte vector accesses (work vectors are allocation-aligned), scalar tail.
 template <class T>
 __global__ void cg_p_kernel(long long n, T* __restrict__ p, const T* __restrict__ z, const SolverState* st) {
+  using V = typename Vec16<T>::type;
+  constexpr int W = Vec16<T>::n;
   if (st->done) return;
   const bool first = st->iter == 1;
   const T beta = (T)st->beta;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+  const long long nv = n / W;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += stride) {
+    V zv = reinterpret_cast<const V*>(z)[i];
+    if (!first) {
+      V pv = reinterpret_cast<const V*>(p)[i];
+      T* pe = reinterpret_cast<T*>(&pv);
+      T* ze = reinterpret_cast<T*>(&zv);
+#pragma unroll
+      for (int k = 0; k < W; k++) ze[k] = axpy_rn(beta, pe[k], ze[k]);
+    }
+    reinterpret_cast<V*>(p)[i] = zv;
+  }
+  for (long long i = nv * W + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride)
     p[i] = first ? z[i] : axpy_rn(beta, p[i], z[i]);
 }
 
@@ -152,9 +218,8 @@ __global__ void __launch_bounds__(kThreads)
     cg_spmv_kernel(SellView<V> A, const T* __restrict__ p, T* __restrict__ q, double* partials,
                    unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (row < A.N) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T y[B];
     sell_row<B, U, V, T>(A, p, row, y);
 #pragma unroll
@@ -172,45 +237,73 @@ __global__ void __launch_bounds__(kThreads)
 
 // X = alpha*P + X; R = -alpha*Q + R; Z = M^-1 R; <R,R>, <R,Z>
 // (CG.f90:89-97 + the next iteration's precond apply and rho).
-// On iterations with iter % 200 == 0 only X is updated here and the residual
-// kernel recomputes R = B - A X.
+// On iterations with iter % iter_RR == 0 only X is updated here and the
+// residual kernel recomputes R = B - A X. Blocks walk tiles of kThreads rows;
+// for B <= 3 a tile's vector segments are staged through shared memory.
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     cg_update_kernel(int N, T* __restrict__ x, const T* __restrict__ p, T* __restrict__ r,
                      const T* __restrict__ q, T* __restrict__ z, const T* __restrict__ alu, int prec,
                      double* partials, unsigned int* ticket, SolverState* st, double* hist) {
+  constexpr bool kStage = B <= 3;
+  constexpr int kS = kStage ? kThreads * B : 1;
+  __shared__ T sx[kS], sp[kS], sr[kS], sq[kS];
   if (st->done) return;
   const bool rr_iter = (st->iter % st->iter_rr) == 0;
   const T alpha = (T)st->alpha;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (row < N) {
-    T t[B];
-#pragma unroll
-    for (int c = 0; c < B; c++) {
-      const long long i = (long long)row * B + c;
-      x[i] = axpy_rn(alpha, p[i], x[i]);
+  const int ntiles = (N + kThreads - 1) / kThreads;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long row0 = (long long)tile * kThreads;
+    const int nrows = (int)min((long long)kThreads, N - row0);
+    const int row = (int)row0 + threadIdx.x;
+    if (kStage) {
+      stage_in<T, B>(sx, x, row0, nrows);
+      stage_in<T, B>(sp, p, row0, nrows);
       if (!rr_iter) {
-        t[c] = axpy_rn(-alpha, q[i], r[i]);
-        r[i] = t[c];
+        stage_in<T, B>(sr, r, row0, nrows);
+        stage_in<T, B>(sq, q, row0, nrows);
       }
+      __syncthreads();
     }
-    if (!rr_iter) {
-      T w[B];
-#pragma unroll
-      for (int c = 0; c < B; c++) w[c] = t[c];
-      if (prec) diag_row<B, T>(alu, N, row, w);
+    if (threadIdx.x < nrows) {
+      T t[B];
 #pragma unroll
       for (int c = 0; c < B; c++) {
-        z[(long long)row * B + c] = w[c];
-        v[0] += (double)t[c] * (double)t[c];
-        v[1] += (double)t[c] * (double)w[c];
+        const int ls = threadIdx.x * B + c;
+        const long long i = (long long)row * B + c;
+        const T xv = axpy_rn(alpha, kStage ? sp[ls] : p[i], kStage ? sx[ls] : x[i]);
+        if (kStage) sx[ls] = xv; else x[i] = xv;
+        if (!rr_iter) t[c] = axpy_rn(-alpha, kStage ? sq[ls] : q[i], kStage ? sr[ls] : r[i]);
       }
+      if (!rr_iter) {
+        T w[B];
+#pragma unroll
+        for (int c = 0; c < B; c++) w[c] = t[c];
+        if (prec) diag_row<B, T>(alu, N, row, w);
+#pragma unroll
+        for (int c = 0; c < B; c++) {
+          const int ls = threadIdx.x * B + c;
+          const long long i = (long long)row * B + c;
+          if (kStage) { sr[ls] = t[c]; sq[ls] = w[c]; } else { r[i] = t[c]; z[i] = w[c]; }
+          v[0] += (double)t[c] * (double)t[c];
+          v[1] += (double)t[c] * (double)w[c];
+        }
+      }
+    }
+    if (kStage) {
+      __syncthreads();
+      stage_out<T, B>(x, sx, row0, nrows);
+      if (!rr_iter) {
+        stage_out<T, B>(r, sr, row0, nrows);
+        stage_out<T, B>(z, sq, row0, nrows);
+      }
+      __syncthreads();
     }
   }
   if (rr_iter) {
-    // iteration counter is not advanced here: the residual kernel that
-    // follows recomputes R = B - A X and finishes the iteration
+    // the counter is not advanced here: the residual kernel that follows
+    // recomputes R = B - A X and finishes the iteration
     if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
     return;
   }
@@ -225,22 +318,47 @@ template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_p_kernel(int N, T* __restrict__ p, const T* __restrict__ r, const T* __restrict__ vv,
                   T* __restrict__ pt, const T* __restrict__ alu, int prec, const SolverState* st) {
+  constexpr bool kStage = B <= 3;
+  constexpr int kS = kStage ? kThreads * B : 1;
+  __shared__ T sp[kS], sr[kS], sv[kS];
   if (st->done) return;
   const bool first = st->iter == 1;
   const T beta = (T)st->beta, omega = (T)st->omega;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= N) return;
-  T w[B];
-#pragma unroll
-  for (int c = 0; c < B; c++) {
-    const long long i = (long long)row * B + c;
-    const T pv = first ? r[i] : add_rn(r[i], mul_rn(beta, sub_rn(p[i], mul_rn(omega, vv[i]))));
-    p[i] = pv;
-    w[c] = pv;
+  const long long row0 = (long long)blockIdx.x * kThreads;
+  const int nrows = (int)min((long long)kThreads, N - row0);
+  const int row = (int)row0 + threadIdx.x;
+  if (kStage) {
+    stage_in<T, B>(sr, r, row0, nrows);
+    if (!first) {
+      stage_in<T, B>(sp, p, row0, nrows);
+      stage_in<T, B>(sv, vv, row0, nrows);
+    }
+    __syncthreads();
   }
-  if (prec) diag_row<B, T>(alu, N, row, w);
+  if (threadIdx.x < nrows) {
+    T w[B];
 #pragma unroll
-  for (int c = 0; c < B; c++) pt[(long long)row * B + c] = w[c];
+    for (int c = 0; c < B; c++) {
+      const int ls = threadIdx.x * B + c;
+      const long long i = (long long)row * B + c;
+      const T rv = kStage ? sr[ls] : r[i];
+      const T pv = first ? rv
+                         : add_rn(rv, mul_rn(beta, sub_rn(kStage ? sp[ls] : p[i], mul_rn(omega, kStage ? sv[ls] : vv[i]))));
+      if (kStage) sp[ls] = pv; else p[i] = pv;
+      w[c] = pv;
+    }
+    if (prec) diag_row<B, T>(alu, N, row, w);
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      if (kStage) sv[threadIdx.x * B + c] = w[c];
+      else pt[(long long)row * B + c] = w[c];
+    }
+  }
+  if (kStage) {
+    __syncthreads();
+    stage_out<T, B>(p, sp, row0, nrows);
+    stage_out<T, B>(pt, sv, row0, nrows);
+  }
 }
 
 // V = A PT; c2 = <RT,V>; alpha = rho/c2 (BiCGSTAB.f90:113-123)
@@ -249,9 +367,8 @@ __global__ void __launch_bounds__(kThreads)
     bicg_v_kernel(SellView<V> A, const T* __restrict__ pt, T* __restrict__ vv, const T* __restrict__ rt,
                   double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[1] = {0.0};
-  if (row < A.N) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T y[B];
     sell_row<B, U, V, T>(A, pt, row, y);
 #pragma unroll
@@ -273,21 +390,41 @@ template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_s_kernel(int N, T* __restrict__ s, const T* __restrict__ r, const T* __restrict__ vv,
                   T* __restrict__ stv, const T* __restrict__ alu, int prec, const SolverState* st) {
+  constexpr bool kStage = B <= 3;
+  constexpr int kS = kStage ? kThreads * B : 1;
+  __shared__ T sr[kS], sv[kS];
   if (st->done) return;
   const T alpha = (T)st->alpha;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= N) return;
-  T w[B];
-#pragma unroll
-  for (int c = 0; c < B; c++) {
-    const long long i = (long long)row * B + c;
-    const T sv = axpy_rn(-alpha, vv[i], r[i]);
-    s[i] = sv;
-    w[c] = sv;
+  const long long row0 = (long long)blockIdx.x * kThreads;
+  const int nrows = (int)min((long long)kThreads, N - row0);
+  const int row = (int)row0 + threadIdx.x;
+  if (kStage) {
+    stage_in<T, B>(sr, r, row0, nrows);
+    stage_in<T, B>(sv, vv, row0, nrows);
+    __syncthreads();
   }
-  if (prec) diag_row<B, T>(alu, N, row, w);
+  if (threadIdx.x < nrows) {
+    T w[B];
 #pragma unroll
-  for (int c = 0; c < B; c++) stv[(long long)row * B + c] = w[c];
+    for (int c = 0; c < B; c++) {
+      const int ls = threadIdx.x * B + c;
+      const long long i = (long long)row * B + c;
+      const T sval = axpy_rn(-alpha, kStage ? sv[ls] : vv[i], kStage ? sr[ls] : r[i]);
+      if (kStage) sr[ls] = sval; else s[i] = sval;
+      w[c] = sval;
+    }
+    if (prec) diag_row<B, T>(alu, N, row, w);
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      if (kStage) sv[threadIdx.x * B + c] = w[c];
+      else stv[(long long)row * B + c] = w[c];
+    }
+  }
+  if (kStage) {
+    __syncthreads();
+    stage_out<T, B>(s, sr, row0, nrows);
+    stage_out<T, B>(stv, sv, row0, nrows);
+  }
 }
 
 // T = A ST; (T,S), (T,T); omega = (T,S)/(T,T) or 0 (BiCGSTAB.f90:128-146)
@@ -296,9 +433,8 @@ __global__ void __launch_bounds__(kThreads)
     bicg_t_kernel(SellView<V> A, const T* __restrict__ stv, T* __restrict__ t, const T* __restrict__ s,
                   double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (row < A.N) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T y[B];
     sell_row<B, U, V, T>(A, stv, row, y);
 #pragma unroll
@@ -317,7 +453,7 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // X = X + alpha*PT + omega*ST; R = -omega*T + S; <R,R>, <R,RT>
-// (BiCGSTAB.f90:148-164). On iter % 200 == 0 only X is updated here.
+// (BiCGSTAB.f90:148-164). On iter % iter_RR == 0 only X is updated here.
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_xr_kernel(int N, T* __restrict__ x, const T* __restrict__ pt, const T* __restrict__ stv,
@@ -345,28 +481,116 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
-// Mixed precision CG: FP32 matrix, vectors and arithmetic in the loop, FP64
-// accumulation of every dot product and FP64 scalars; FP64 solution x and an
-// FP64 true residual r = b - A x recomputed ("reliable update") whenever the
-// iterated residual has dropped by `delta` since the last refresh, or looks
-// converged. The Krylov direction p is kept across refreshes.
+// Mixed precision CG: FP32 matrix (paired layout), vectors and arithmetic in
+// the loop; FP64 accumulation of every dot product and FP64 scalars. The
+// FP64 solution is x + y, with y the FP32 correction accumulated since the
+// last refresh. When the iterated residual norm has dropped below `delta`
+// times its largest value since the last refresh (which bounds the range
+// that y and the FP32 recursion must carry), when `period` iterations have
+// passed without one, or when it looks converged, the solver recomputes
+// r = b - A (x + y) with the FP64 matrix and continues from it with the same
+// search direction p ("reliable update", Sleijpen & van der Vorst 1996).
+// Convergence is decided only on that FP64 residual. The fold x += y, y = 0
+// is done by the next p update (or after the loop).
 // ---------------------------------------------------------------------------
 __device__ void fin_mixed_inner(SolverState* st, double rr, double rz, double* hist) {
   const double rn = sqrt(rr);
   const double resid = sqrt(rr / st->B2);
   record(st, hist, resid);
+  st->rho1 = st->rho;
   if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
   if (rn > st->rmax) st->rmax = rn;
-  if (rn < st->delta * st->rmax || resid < st->tol || st->iter >= st->max_iter) {
-    st->refresh = 1;  // the refresh kernels finish this iteration
-    st->rho1 = st->rho;
-    st->rr = rz;      // kept in case the refresh is the last step
+  if (rn < st->delta * st->rmax || resid < st->tol || st->iter >= st->max_iter ||
+      (st->period > 0 && st->iter - st->last_refresh >= st->period)) {
+    st->refresh = 1;  // the refresh kernel of this iteration finishes it
     return;
   }
-  st->rho1 = st->rho;
   st->rho = rz;
   st->beta = st->rho / st->rho1;
   st->iter += 1;
+}
+
+// P = Z + beta*P in FP32 (P = Z on iteration 1), and after a refresh the
+// fold of the FP32 correction into the FP64 solution: X += Y, Y = 0.
+__global__ void mixed_p_kernel(long long n, float* __restrict__ p, const float* __restrict__ z,
+                               double* __restrict__ x, float* __restrict__ y, const SolverState* st) {
+  if (st->done) return;
+  const bool first = st->iter == 1;
+  const bool fold = st->fold != 0;
+  const float beta = (float)st->beta;
+  const bool xal = (reinterpret_cast<uintptr_t>(x) & 15) == 0;
+  const long long nv = n / 4;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += stride) {
+    float4 zv = reinterpret_cast<const float4*>(z)[i];
+    if (!first) {
+      const float4 pv = reinterpret_cast<const float4*>(p)[i];
+      zv.x = fmaf(beta, pv.x, zv.x);
+      zv.y = fmaf(beta, pv.y, zv.y);
+      zv.z = fmaf(beta, pv.z, zv.z);
+      zv.w = fmaf(beta, pv.w, zv.w);
+    }
+    reinterpret_cast<float4*>(p)[i] = zv;
+    if (fold) {
+      const float4 yv = reinterpret_cast<const float4*>(y)[i];
+      if (xal) {
+        double2 a = reinterpret_cast<double2*>(x)[2 * i];
+        double2 b = reinterpret_cast<double2*>(x)[2 * i + 1];
+        a.x += (double)yv.x;
+        a.y += (double)yv.y;
+        b.x += (double)yv.z;
+        b.y += (double)yv.w;
+        reinterpret_cast<double2*>(x)[2 * i] = a;
+        reinterpret_cast<double2*>(x)[2 * i + 1] = b;
+      } else {
+        x[4 * i] += (double)yv.x;
+        x[4 * i + 1] += (double)yv.y;
+        x[4 * i + 2] += (double)yv.z;
+        x[4 * i + 3] += (double)yv.w;
+      }
+      reinterpret_cast<float4*>(y)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+  }
+  for (long long i = nv * 4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
+    p[i] = first ? z[i] : fmaf(beta, p[i], z[i]);
+    if (fold) {
+      x[i] += (double)y[i];
+      y[i] = 0.0f;
+    }
+  }
+}
+
+// FP32 paired-layout SpMV fused with <P,Q> (mixed precision inner loop).
+template <int B, int U>
+__global__ void __launch_bounds__(kThreads)
+    cg_spmv2_kernel(SellView2 A, const float* __restrict__ p, float* __restrict__ q, double* partials,
+                    unsigned int* ticket, SolverState* st) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  const int npairs = (A.N + 1) / 2;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+    float y0[B], y1[B];
+    sell_row2<B, U>(A, p, t, y0, y1);
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = (long long)2 * t * B + c;
+      q[i] = y0[c];
+      v[0] += (double)p[i] * (double)y0[c];
+    }
+    if (2 * t + 1 < A.N) {
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        const long long i = (long long)(2 * t + 1) * B + c;
+        q[i] = y1[c];
+        v[0] += (double)p[i] * (double)y1[c];
+      }
+    }
+  }
+  grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    st->omega = tot[0];
+    st->alpha = st->rho / tot[0];
+    st->fold = 0;  // the p kernel of this iteration has folded y
+  });
 }
 
 // y += alpha*p; r -= alpha*q; z = M^-1 r; dots (FP32 vectors, FP64 sums)
@@ -375,47 +599,89 @@ __global__ void __launch_bounds__(kThreads)
     mixed_update_kernel(int N, float* __restrict__ y, const float* __restrict__ p, float* __restrict__ r,
                         const float* __restrict__ q, float* __restrict__ z, const float* __restrict__ alu, int prec,
                         double* partials, unsigned int* ticket, SolverState* st, double* hist) {
+  constexpr bool kStage = B <= 3;
+  constexpr int kS = kStage ? kThreads * B : 1;
+  __shared__ float sy[kS], sp[kS], sr[kS], sq[kS];
   if (st->done) return;
   const float alpha = (float)st->alpha;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (row < N) {
-    float t[B], w[B];
-#pragma unroll
-    for (int c = 0; c < B; c++) {
-      const long long i = (long long)row * B + c;
-      y[i] = fmaf(alpha, p[i], y[i]);
-      t[c] = fmaf(-alpha, q[i], r[i]);
-      r[i] = t[c];
-      w[c] = t[c];
+  const int ntiles = (N + kThreads - 1) / kThreads;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const long long row0 = (long long)tile * kThreads;
+    const int nrows = (int)min((long long)kThreads, N - row0);
+    const int row = (int)row0 + threadIdx.x;
+    if (kStage) {
+      stage_in<float, B>(sy, y, row0, nrows);
+      stage_in<float, B>(sp, p, row0, nrows);
+      stage_in<float, B>(sr, r, row0, nrows);
+      stage_in<float, B>(sq, q, row0, nrows);
+      __syncthreads();
     }
-    if (prec) diag_row<B, float>(alu, N, row, w);
+    if (threadIdx.x < nrows) {
+      float t[B], w[B];
 #pragma unroll
-    for (int c = 0; c < B; c++) {
-      z[(long long)row * B + c] = w[c];
-      v[0] += (double)t[c] * (double)t[c];
-      v[1] += (double)t[c] * (double)w[c];
+      for (int c = 0; c < B; c++) {
+        const int ls = threadIdx.x * B + c;
+        const long long i = (long long)row * B + c;
+        const float yv = fmaf(alpha, kStage ? sp[ls] : p[i], kStage ? sy[ls] : y[i]);
+        if (kStage) sy[ls] = yv; else y[i] = yv;
+        t[c] = fmaf(-alpha, kStage ? sq[ls] : q[i], kStage ? sr[ls] : r[i]);
+        w[c] = t[c];
+      }
+      if (prec) diag_row<B, float>(alu, N, row, w);
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        const int ls = threadIdx.x * B + c;
+        const long long i = (long long)row * B + c;
+        if (kStage) { sr[ls] = t[c]; sq[ls] = w[c]; } else { r[i] = t[c]; z[i] = w[c]; }
+        v[0] += (double)t[c] * (double)t[c];
+        v[1] += (double)t[c] * (double)w[c];
+      }
+    }
+    if (kStage) {
+      __syncthreads();
+      stage_out<float, B>(y, sy, row0, nrows);
+      stage_out<float, B>(r, sr, row0, nrows);
+      stage_out<float, B>(z, sq, row0, nrows);
+      __syncthreads();
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_mixed_inner(st, tot[0], tot[1], hist); });
 }
 
-// Refresh step: x += y (FP64), y = 0, r64 = b - A64 x, r = fp32(r64),
-// z = M^-1 r; dots <r64,r64> (true residual) and <r,z>. Also the initial
-// residual when iter == 0. Runs only when st->refresh or iter == 0.
-template <int B, int U>
+// Refresh: r64 = b - A64 (x + y) with the FP64 matrix, r = fp32(r64),
+// z = M^-1 r; dots <r64,r64> (the true residual) and <r,z>. Runs for the
+// initial residual (iter == 0) and when the update kernel raised `refresh`;
+// it sits in every iteration on a small grid, so the common case (nothing
+// to do) costs one flag read per block.
+template <int B>
 __global__ void __launch_bounds__(kThreads)
-    mixed_resid_kernel(SellView<double> A, double* __restrict__ x, const double* __restrict__ b,
-                       float* __restrict__ y, float* __restrict__ r, float* __restrict__ z,
-                       const float* __restrict__ alu, int prec, double* partials, unsigned int* ticket,
-                       SolverState* st, double* hist) {
-  if (st->done) return;
-  if (!(st->refresh || st->iter == 0)) return;
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    mixed_refresh_kernel(SellView<double> A, const double* __restrict__ x, const float* __restrict__ y,
+                         const double* __restrict__ b, float* __restrict__ r, float* __restrict__ z,
+                         const float* __restrict__ alu, int prec, double* partials, unsigned int* ticket,
+                         SolverState* st, double* hist) {
+  if (st->done || !(st->iter == 0 || st->refresh)) return;
+  constexpr int B2 = B * B;
   double v[2] = {0.0, 0.0};
-  if (row < A.N) {
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+    // (A (x + y))[row] in FP64, blocks in CSR order
+    const int lane = row & (kSlice - 1);
+    const long long base = A.slptr[row >> 5];
+    const int len = A.rowptr[row + 1] - A.rowptr[row];
     double ax[B];
-    sell_row<B, U, double, double>(A, x, row, ax);
+#pragma unroll
+    for (int c = 0; c < B; c++) ax[c] = 0.0;
+    for (int k = 0; k < len; k++) {
+      const int j = ld_stream(A.col + base + lane + (long long)k * kSlice);
+      double xs[B];
+#pragma unroll
+      for (int l = 0; l < B; l++) xs[l] = x[(long long)j * B + l] + (double)y[(long long)j * B + l];
+      const double* vk = A.val + (base + (long long)k * kSlice) * B2 + lane;
+#pragma unroll
+      for (int q = 0; q < B; q++)
+#pragma unroll
+        for (int l = 0; l < B; l++) ax[q] = fma(ld_stream(vk + (q * B + l) * kSlice), xs[l], ax[q]);
+    }
     float t[B], w[B];
 #pragma unroll
     for (int c = 0; c < B; c++) {
@@ -425,7 +691,6 @@ __global__ void __launch_bounds__(kThreads)
       t[c] = (float)rv;
       r[i] = t[c];
       w[c] = t[c];
-      y[i] = 0.0f;
     }
     if (prec) diag_row<B, float>(alu, A.N, row, w);
 #pragma unroll
@@ -447,7 +712,9 @@ __global__ void __launch_bounds__(kThreads)
     const double resid = sqrt(rr / st->B2);
     record(st, hist, resid);
     st->refresh = 0;
+    st->fold = 1;
     st->n_refine += 1;
+    st->last_refresh = st->iter;
     if (resid < st->tol) { st->done = 1; st->status = kOk; return; }
     if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
     if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
@@ -458,13 +725,13 @@ __global__ void __launch_bounds__(kThreads)
   });
 }
 
-// x += y before the refresh residual (separate pass: the residual kernel
-// reads x at neighbouring rows).
-__global__ void mixed_fold_kernel(long long n, double* __restrict__ x, const float* __restrict__ y,
-                                  const SolverState* st) {
-  if (st->done || !st->refresh) return;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+// Final fold x += y after the loop (the solution is x + y).
+__global__ void mixed_fold_kernel(long long n, double* __restrict__ x, float* __restrict__ y, const SolverState* st) {
+  if (!st->fold) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     x[i] += (double)y[i];
+    y[i] = 0.0f;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -483,10 +750,14 @@ int dispatch_ndof(int ndof, F&& f) {
   }
 }
 
-template <int B>
-struct Unroll {
-  static constexpr int value = B == 1 ? 4 : (B <= 3 ? 2 : 1);
-};
+template <class F>
+int dispatch_u(int u, F&& f) {
+  switch (u) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    default: return f(std::integral_constant<int, 2>{});
+  }
+}
 
 struct Vecs {
   std::vector<void*> ptrs;
@@ -502,6 +773,23 @@ struct Vecs {
     return static_cast<T*>(p);
   }
 };
+
+// One solver as kernel launch sequences.
+struct Plan {
+  // enqueue one iteration; `special` adds the true-residual kernel (FP64);
+  // ev (nullable) receives an event before and after every kernel slot
+  std::function<void(cudaStream_t, cudaEvent_t*, bool special)> iteration;
+  std::function<void(cudaStream_t)> finalize;  // mixed: final fold
+  int kernels = 0;         // kernel slots of an iteration (FP64: the last is the special kernel)
+  bool always_all = false; // every slot launches every iteration (mixed)
+  std::vector<int> kind;   // per slot: 0 SpMV, 1 other vector kernel, 2 precond-applying kernel
+};
+
+int largest_divisor_at_most(int v, int cap) {
+  for (int d = cap; d > 1; d--)
+    if (v % d == 0) return d;
+  return 1;
+}
 
 }  // namespace
 
@@ -523,10 +811,23 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     if (rc) return rc;
   }
 
+  const int iter_rr = p.iter_rr > 0 ? p.iter_rr : 200;
+  // Iterations per graph launch. FP64: the replacement iterations must fall
+  // on the last iteration of a batch, so the batch divides iter_RR.
+  int batch, period;
+  if (p.precision == 1) {
+    batch = p.batch > 0 ? p.batch : 16;
+    period = 0;  // refreshes are decided on the device
+  } else {
+    period = iter_rr;
+    batch = p.batch > 0 && iter_rr % p.batch == 0 ? p.batch : largest_divisor_at_most(iter_rr, 25);
+  }
+
   SolverState h{};
   h.tol = p.tol;
   h.max_iter = p.max_iter;
-  h.iter_rr = p.iter_rr > 0 ? p.iter_rr : 200;
+  h.iter_rr = iter_rr;
+  h.period = p.precision == 1 ? p.refresh_period : 0;
   h.delta = p.delta > 0 ? p.delta : 0.1;
   MB_CUDA_OK(cudaMemcpyAsync(sc.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
   MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * 64, s));
@@ -534,159 +835,235 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
 
   Vecs vec{{}, s};
   const int gb = blocks_for(N);
-  std::function<void(cudaStream_t)> iteration;
-  int kernels_per_iter = 0;
+  Plan plan;
   auto t0 = std::chrono::steady_clock::now();
 
   rc = dispatch_ndof(nd, [&](auto Bc) -> int {
-    constexpr int B = decltype(Bc)::value;
-    constexpr int U = Unroll<B>::value;
+   constexpr int B = decltype(Bc)::value;
+   return dispatch_u(p.precision == 0 ? m.u64 : m.u32, [&](auto Uc) -> int {
+    constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
     SellView<double> A64 = view_of<double>(m);
     double* partials = sc.partials;
     unsigned int* ticket = sc.ticket;
     SolverState* st = sc.st;
     double* hist = sc.hist;
+    const int gvec = num_sms() * 8;
     if (p.precision == 0) {
       const double* alu = m.d_alu64;
+      double* x = d_x;
+      const double* b = d_b;
+      auto k_resid = resid_kernel<B, U, double, double>;
+      const int g_resid = pgrid(k_resid);
       if (p.method == 1) {
         double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n), *pp = vec.get<double>(n);
         if (!r || !z || !q || !pp) return kCudaError;
-        double* x = d_x;
-        const double* b = d_b;
-        resid_kernel<B, U, double, double><<<gb, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, 0,
-                                                                   partials, ticket, st, hist);
-        kernels_per_iter = 4;
-        iteration = [=](cudaStream_t ss) {
-          cg_p_kernel<double><<<kVecBlocks, kThreads, 0, ss>>>(n, pp, z, st);
-          cg_spmv_kernel<B, U, double, double><<<gb, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st);
-          cg_update_kernel<B, double><<<gb, kThreads, 0, ss>>>(N, x, pp, r, q, z, alu, prec, partials, ticket, st,
-                                                               hist);
-          resid_kernel<B, U, double, double><<<gb, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, 1,
-                                                                      partials, ticket, st, hist);
+        auto k_spmv = cg_spmv_kernel<B, U, double, double>;
+        auto k_upd = cg_update_kernel<B, double>;
+        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
+        plan.kernels = 4;
+        plan.kind = {1, 0, 2, 0};
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          cg_p_kernel<double><<<gvec, kThreads, 0, ss>>>(n, pp, z, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[2], ss);
+          k_upd<<<g_upd, kThreads, 0, ss>>>(N, x, pp, r, q, z, alu, prec, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[3], ss);
+          if (special) k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket,
+                                                             st, hist);
+          if (ev) cudaEventRecord(ev[4], ss);
         };
       } else {
         double *r = vec.get<double>(n), *rt = vec.get<double>(n), *pp = vec.get<double>(n),
                *pt = vec.get<double>(n), *sv = vec.get<double>(n), *stv = vec.get<double>(n),
                *t = vec.get<double>(n), *vv = vec.get<double>(n);
         if (!r || !rt || !pp || !pt || !sv || !stv || !t || !vv) return kCudaError;
-        double* x = d_x;
-        const double* b = d_b;
-        resid_kernel<B, U, double, double><<<gb, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, 0,
-                                                                   partials, ticket, st, hist);
-        kernels_per_iter = 6;
-        iteration = [=](cudaStream_t ss) {
+        auto k_v = bicg_v_kernel<B, U, double, double>;
+        auto k_t = bicg_t_kernel<B, U, double, double>;
+        auto k_xr = bicg_xr_kernel<B, double>;
+        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
+        plan.kernels = 6;
+        plan.kind = {2, 0, 2, 0, 1, 0};
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
           bicg_p_kernel<B, double><<<gb, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
-          bicg_v_kernel<B, U, double, double><<<gb, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[2], ss);
           bicg_s_kernel<B, double><<<gb, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
-          bicg_t_kernel<B, U, double, double><<<gb, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
-          bicg_xr_kernel<B, double><<<kVecBlocks, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket,
-                                                                     st, hist);
-          resid_kernel<B, U, double, double><<<gb, kThreads, 0, ss>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, 1,
-                                                                      partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[3], ss);
+          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[4], ss);
+          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[5], ss);
+          if (special) k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket,
+                                                             st, hist);
+          if (ev) cudaEventRecord(ev[6], ss);
         };
       }
     } else {
-      SellView<float> A32 = view_of<float>(m);
+      SellView2 A32 = view2_of(m);
       const float* alu32 = m.d_alu32;
       float *r = vec.get<float>(n), *z = vec.get<float>(n), *q = vec.get<float>(n), *pp = vec.get<float>(n),
             *y = vec.get<float>(n);
       if (!r || !z || !q || !pp || !y) return kCudaError;
       double* x = d_x;
       const double* b = d_b;
-      mixed_resid_kernel<B, U><<<gb, kThreads, 0, s>>>(A64, x, b, y, r, z, alu32, prec, partials, ticket, st, hist);
-      kernels_per_iter = 5;
-      iteration = [=](cudaStream_t ss) {
-        cg_p_kernel<float><<<kVecBlocks, kThreads, 0, ss>>>(n, pp, z, st);
-        cg_spmv_kernel<B, Unroll<B>::value + 1, float, float><<<gb, kThreads, 0, ss>>>(A32, pp, q, partials, ticket,
-                                                                                    st);
-        mixed_update_kernel<B><<<gb, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist);
-        mixed_fold_kernel<<<kVecBlocks, kThreads, 0, ss>>>(n, x, y, st);
-        mixed_resid_kernel<B, U><<<gb, kThreads, 0, ss>>>(A64, x, b, y, r, z, alu32, prec, partials, ticket, st,
-                                                          hist);
+      auto k_spmv = cg_spmv2_kernel<B, U>;
+      auto k_upd = mixed_update_kernel<B>;
+      auto k_ref = mixed_refresh_kernel<B>;
+      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+      const int g_ref = 2 * num_sms();  // mostly a no-op: small grid
+      if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
+      k_ref<<<pgrid(k_ref), kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
+      plan.kernels = 4;
+      plan.always_all = true;
+      plan.kind = {1, 0, 2, 0};
+      plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
+        if (ev) cudaEventRecord(ev[0], ss);
+        mixed_p_kernel<<<gvec, kThreads, 0, ss>>>(n, pp, z, x, y, st);
+        if (ev) cudaEventRecord(ev[1], ss);
+        k_spmv<<<g_spmv, kThreads, 0, ss>>>(A32, pp, q, partials, ticket, st);
+        if (ev) cudaEventRecord(ev[2], ss);
+        k_upd<<<g_upd, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist);
+        if (ev) cudaEventRecord(ev[3], ss);
+        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
+        if (ev) cudaEventRecord(ev[4], ss);
       };
+      plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n, x, y, st); };
     }
     return kOk;
+   });
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
-
-  // Batches of iterations, captured once into a graph.
-  const int batch = p.batch > 0 ? p.batch : 16;
-  cudaGraphExec_t exec = nullptr;
-  if (p.use_graph) {
-    cudaGraph_t g = nullptr;
-    MB_CUDA_OK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < batch; k++) iteration(s);
-    MB_CUDA_OK(cudaStreamEndCapture(s, &g));
-    MB_CUDA_OK(cudaGraphInstantiate(&exec, g, 0));
-    cudaGraphDestroy(g);
-  }
-  auto launch_batch = [&]() -> cudaError_t {
-    if (exec) return cudaGraphLaunch(exec, s);
-    for (int k = 0; k < batch; k++) iteration(s);
-    return cudaGetLastError();
+  long long launched_kernels = 1;
+  auto kernels_of = [&](bool special) -> long long {
+    return plan.kernels - ((special || plan.always_all) ? 0 : 1);
   };
-  cudaEvent_t ev[2];
-  cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-  cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
-  const long long max_batches = (long long)p.max_iter / batch + 4;
-  int cur = 0;
-  long long launched = 0;
-  bool finished = false;
-  cudaError_t err = cudaSuccess;
-  // prime: two batches in flight
-  for (int k = 0; k < 2 && !finished; k++) {
-    err = launch_batch();
-    if (err != cudaSuccess) break;
-    cudaMemcpyAsync(&sc.h_st[k], sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
-    cudaEventRecord(ev[k], s);
-    launched++;
-  }
-  while (err == cudaSuccess && !finished) {
-    err = cudaEventSynchronize(ev[cur]);
-    if (err != cudaSuccess) break;
-    if (sc.h_st[cur].done || launched > max_batches) {
-      finished = true;
-      break;
-    }
-    err = launch_batch();
-    if (err != cudaSuccess) break;
-    cudaMemcpyAsync(&sc.h_st[cur], sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
-    cudaEventRecord(ev[cur], s);
-    launched++;
-    cur ^= 1;
-  }
-  cudaError_t e2 = cudaStreamSynchronize(s);
-  if (err == cudaSuccess) err = e2;
-  cudaEventDestroy(ev[0]);
-  cudaEventDestroy(ev[1]);
-  if (exec) cudaGraphExecDestroy(exec);
-  if (err != cudaSuccess) return report_cuda(err, "solver loop", __FILE__, __LINE__);
 
-  SolverState fin{};
-  MB_CUDA_OK(cudaMemcpy(&fin, sc.st, sizeof(fin), cudaMemcpyDeviceToHost));
-  res.t_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  if (!fin.done) {
-    fprintf(stderr, "** monolis_b200: solver loop ended without a verdict\n");
-    fin.status = kTimeout;
-  }
-  if (fin.status == kZeroRhs) {
-    fprintf(stderr, "** monolis error: norm of RHS vector B is 0.0\n");
-    MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n, s));
-    MB_CUDA_OK(cudaStreamSynchronize(s));
-    res.iter = 0;
-    res.status = kOk;
-    res.resid = 0.0;
+  auto finish = [&](SolverState fin) -> int {
+    if (!fin.done) {
+      fprintf(stderr, "** monolis_b200: solver loop ended without a verdict\n");
+      fin.status = kTimeout;
+    }
+    if (fin.status == kZeroRhs) {
+      fprintf(stderr, "** monolis error: norm of RHS vector B is 0.0\n");
+      MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n, s));
+      MB_CUDA_OK(cudaStreamSynchronize(s));
+      res.iter = 0;
+      res.status = kOk;
+      res.resid = 0.0;
+      return kOk;
+    }
+    res.iter = fin.iter;
+    res.status = fin.status;
+    res.resid = fin.resid;
+    res.n_refine = fin.n_refine;
+    res.launches = launched_kernels;
+    if (h_hist && fin.iter > 0)
+      MB_CUDA_OK(cudaMemcpy(h_hist, sc.hist, sizeof(double) * ((size_t)fin.iter + 1), cudaMemcpyDeviceToHost));
     return kOk;
+  };
+  auto is_special = [&](long long it) { return period > 0 && it > 0 && it % period == 0; };
+  auto read_state = [&](SolverState& out) -> cudaError_t {
+    cudaError_t e = cudaMemcpyAsync(sc.h_st, sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    out = sc.h_st[0];
+    return e;
+  };
+
+  res.kernel_time.assign(plan.kernels, 0.0);
+  SolverState cur{};
+  cudaError_t err = read_state(cur);
+  if (err != cudaSuccess) return report_cuda(err, "solver init", __FILE__, __LINE__);
+  const long long iter_cap = (long long)p.max_iter + 4 * (long long)batch + 8;
+
+  if (p.timers) {
+    // Timing mode: no graph; events around every kernel, one iteration at a
+    // time (the host waits for each iteration, so the loop itself is slower).
+    std::vector<cudaEvent_t> tev(plan.kernels + 1);
+    for (auto& e : tev) cudaEventCreate(&e);
+    long long its = 0;
+    while (err == cudaSuccess && !cur.done && its++ <= iter_cap) {
+      const bool special = is_special(cur.iter);
+      plan.iteration(s, tev.data(), special);
+      launched_kernels += kernels_of(special);
+      err = read_state(cur);
+      if (err != cudaSuccess) break;
+      for (int k = 0; k < plan.kernels; k++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, tev[k], tev[k + 1]);
+        res.kernel_time[k] += ms * 1e-3;
+      }
+    }
+    for (auto& e : tev) cudaEventDestroy(e);
+    if (err != cudaSuccess) return report_cuda(err, "solver loop (timers)", __FILE__, __LINE__);
+    for (int k = 0; k < plan.kernels; k++) res.t_kind[plan.kind[k]] += res.kernel_time[k];
+  } else if (!cur.done) {
+    // Two graphs of `batch` iterations: plain, and with the true-residual
+    // kernel in the last iteration (FP64 only).
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    const int ngraphs = period > 0 ? 2 : 1;
+    if (p.use_graph) {
+      for (int g = 0; g < ngraphs; g++) {
+        cudaGraph_t graph = nullptr;
+        MB_CUDA_OK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < batch; k++) plan.iteration(s, nullptr, g == 1 && k == batch - 1);
+        MB_CUDA_OK(cudaStreamEndCapture(s, &graph));
+        MB_CUDA_OK(cudaGraphInstantiate(&exec[g], graph, 0));
+        cudaGraphDestroy(graph);
+      }
+    }
+    cudaEvent_t ev[2];
+    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    long long next = cur.iter;  // iteration the next enqueued batch starts with (batches start at 1 mod batch)
+    int inflight = 0, slot = 0;
+    while (err == cudaSuccess) {
+      const int special = is_special(next + batch - 1) ? 1 : 0;
+      if (exec[special]) {
+        err = cudaGraphLaunch(exec[special], s);
+      } else {
+        for (int k = 0; k < batch; k++) plan.iteration(s, nullptr, special && k == batch - 1);
+        err = cudaGetLastError();
+      }
+      if (err != cudaSuccess) break;
+      launched_kernels += (long long)(batch - 1) * kernels_of(false) + kernels_of(special);
+      next += batch;
+      cudaMemcpyAsync(&sc.h_st[slot], sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
+      cudaEventRecord(ev[slot], s);
+      slot ^= 1;
+      if (++inflight < 2) continue;
+      err = cudaEventSynchronize(ev[slot]);  // the older launch
+      if (err != cudaSuccess) break;
+      inflight--;
+      if (sc.h_st[slot].done) break;
+      if (next > iter_cap) {
+        fprintf(stderr, "** monolis_b200: iteration cap reached without a verdict\n");
+        break;
+      }
+    }
+    cudaError_t e2 = cudaStreamSynchronize(s);
+    if (err == cudaSuccess) err = e2;
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    for (auto& e : exec)
+      if (e) cudaGraphExecDestroy(e);
+    if (err != cudaSuccess) return report_cuda(err, "solver loop", __FILE__, __LINE__);
   }
-  res.launches = 1 + launched * batch * kernels_per_iter;
-  res.iter = fin.iter;
-  res.status = fin.status;
-  res.resid = fin.resid;
-  res.n_refine = fin.n_refine;
-  if (h_hist && fin.iter > 0)
-    MB_CUDA_OK(cudaMemcpy(h_hist, sc.hist, sizeof(double) * ((size_t)fin.iter + 1), cudaMemcpyDeviceToHost));
-  return kOk;
+  if (plan.finalize) {
+    plan.finalize(s);
+    launched_kernels += 1;
+  }
+  SolverState fin{};
+  err = read_state(fin);
+  if (err != cudaSuccess) return report_cuda(err, "solver final state", __FILE__, __LINE__);
+  res.t_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return finish(fin);
 }
 
 }  // namespace mb

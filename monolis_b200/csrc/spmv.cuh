@@ -22,10 +22,6 @@ template <>
 inline SellView<double> view_of<double>(const SellMatrix& m) {
   return {m.d_rowptr, m.d_slptr, m.d_col, m.d_val64, m.N};
 }
-template <>
-inline SellView<float> view_of<float>(const SellMatrix& m) {
-  return {m.d_rowptr, m.d_slptr, m.d_col, m.d_val32, m.N};
-}
 
 // y = (A x)[row] for one block row, blocks visited in CSR order. Within a
 // block the reference evaluates Y_r = ((Y_r + a_r0*x0) + a_r1*x1) + a_r2*x2
@@ -76,6 +72,103 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
 #pragma unroll
       for (int l = 0; l < B; l++) y[r] = add_rn(y[r], mul_rn(T(a[r * B + l]), xs[l]));
   }
+}
+
+// Paired FP32 layout (see SellMatrix::d_col2): thread t owns rows 2t and
+// 2t+1 of the matrix; slot k of its pair is at block slptr2[t/32] + 64k + 2(t%32).
+struct SellView2 {
+  const int* __restrict__ rowptr;
+  const long long* __restrict__ slptr2;
+  const int* __restrict__ col2;
+  const float* __restrict__ val;
+  int N;
+};
+
+inline SellView2 view2_of(const SellMatrix& m) { return {m.d_rowptr, m.d_slptr2, m.d_col2, m.d_val32, m.N}; }
+
+__device__ __forceinline__ float2 ld_stream2(const float2* p) { return __ldcs(p); }
+__device__ __forceinline__ int2 ld_stream2(const int2* p) { return __ldcs(p); }
+
+// y0/y1 = (A x) of rows 2t and 2t+1 in FP32 (fused multiply-add). Slots past
+// a row's length hold zero values and a valid column, so both rows run to the
+// longer length.
+template <int B, int U>
+__device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
+                                          float (&y1)[B]) {
+  constexpr int B2 = B * B;
+  const int r0 = 2 * t;
+  const int lane2 = 2 * (t & 31);
+  const long long base = A.slptr2[t >> 5];
+  const int len0 = A.rowptr[r0 + 1] - A.rowptr[r0];
+  const int len1 = (r0 + 1 < A.N) ? A.rowptr[r0 + 2] - A.rowptr[r0 + 1] : 0;
+  const int len = len0 > len1 ? len0 : len1;
+  const int2* __restrict__ c = reinterpret_cast<const int2*>(A.col2 + base + lane2);
+  const float2* __restrict__ v = reinterpret_cast<const float2*>(A.val + base * B2 + lane2);
+#pragma unroll
+  for (int r = 0; r < B; r++) { y0[r] = 0.f; y1[r] = 0.f; }
+  int k = 0;
+  for (; k + U <= len; k += U) {
+    int2 j[U];
+    float2 a[U][B2];
+#pragma unroll
+    for (int u = 0; u < U; u++) j[u] = ld_stream2(c + (long long)(k + u) * 32);
+#pragma unroll
+    for (int u = 0; u < U; u++)
+#pragma unroll
+      for (int e = 0; e < B2; e++) a[u][e] = ld_stream2(v + ((long long)(k + u) * B2 + e) * 32);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      float x0[B], x1[B];
+#pragma unroll
+      for (int l = 0; l < B; l++) {
+        x0[l] = __ldg(x + (long long)j[u].x * B + l);
+        x1[l] = __ldg(x + (long long)j[u].y * B + l);
+      }
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int l = 0; l < B; l++) {
+          y0[r] = fmaf(a[u][r * B + l].x, x0[l], y0[r]);
+          y1[r] = fmaf(a[u][r * B + l].y, x1[l], y1[r]);
+        }
+    }
+  }
+  for (; k < len; k++) {
+    const int2 jj = ld_stream2(c + (long long)k * 32);
+    float2 a[B2];
+#pragma unroll
+    for (int e = 0; e < B2; e++) a[e] = ld_stream2(v + ((long long)k * B2 + e) * 32);
+    float x0[B], x1[B];
+#pragma unroll
+    for (int l = 0; l < B; l++) {
+      x0[l] = __ldg(x + (long long)jj.x * B + l);
+      x1[l] = __ldg(x + (long long)jj.y * B + l);
+    }
+#pragma unroll
+    for (int r = 0; r < B; r++)
+#pragma unroll
+      for (int l = 0; l < B; l++) {
+        y0[r] = fmaf(a[r * B + l].x, x0[l], y0[r]);
+        y1[r] = fmaf(a[r * B + l].y, x1[l], y1[r]);
+      }
+  }
+}
+
+// Block-cooperative staging of the entries of an interleaved vector
+// (x[row*B + c]) that belong to a tile of rows: global memory is read and
+// written as contiguous runs (coalesced), threads then work on whole rows in
+// shared memory. Used for B <= 3; larger blocks access global memory directly.
+template <class T, int B>
+__device__ __forceinline__ void stage_in(T* s, const T* __restrict__ g, long long row0, int nrows) {
+  const long long base = row0 * B;
+  const int len = nrows * B;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) s[i] = g[base + i];
+}
+template <class T, int B>
+__device__ __forceinline__ void stage_out(T* __restrict__ g, const T* s, long long row0, int nrows) {
+  const long long base = row0 * B;
+  const int len = nrows * B;
+  for (int i = threadIdx.x; i < len; i += blockDim.x) g[base + i] = s[i];
 }
 
 // z = M^-1 v for one block row with the in-place LU factors of the diagonal

@@ -33,6 +33,35 @@ def test_spmv_bit_exact(gpu, oracle, problem, kw):
         assert bits_equal(yp, yo)
 
 
+@pytest.mark.parametrize("problem,kw", [
+    ("elasticity", dict(n=9)),
+    ("convection_diffusion", dict(n=13, peclet=5.0)),
+    ("laplacian", dict(n=11)),
+])
+def test_spmv_fp32_paired_layout(gpu, oracle, problem, kw):
+    """FP32 SpMV (paired layout, FMA) against the oracle's FP64 SpMV of the
+    same FP32-rounded inputs: per row |y32 - y| <= 1e-6 * (|A| |x|)."""
+    import torch
+    mp, b = build(gpu, problem, **kw)
+    mo, _ = build(oracle, problem, **kw)
+    mp.set_precision(1)
+    mp.device_prepare()
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(len(b)).astype(np.float32)
+    vals32 = mo.values().astype(np.float32).astype(np.float64)
+    mo_abs, _ = build(oracle, problem, **kw)
+    mo_abs.values()[:] = np.abs(vals32)
+    bound = mo_abs.matvec(np.abs(x.astype(np.float64)))
+    mo.values()[:] = vals32
+    y_ref = mo.matvec(x.astype(np.float64))
+    d_x = torch.from_numpy(x).cuda()
+    d_y = torch.empty_like(d_x)
+    mp.device_matvec(d_x.data_ptr(), d_y.data_ptr(), fp32=True)
+    torch.cuda.synchronize()
+    y32 = d_y.cpu().numpy().astype(np.float64)
+    assert np.all(np.abs(y32 - y_ref) <= 1e-6 * bound + 1e-30)
+
+
 def test_spmv_ndof2_random_blocks(gpu, oracle):
     # 10-node chain, ndof 2, like wrapper_test/solver/monolis_solver_c_test.c
     elem = np.array([[i, i + 1] for i in range(9)], dtype=np.int32)
@@ -134,6 +163,17 @@ def test_bicgstab_chaotic_cases_converge(gpu, oracle, problem, kw, method, prec,
     assert st_o == 0 and st_p == 0 and res_p < tol
     assert abs(it_p - it_o) <= 0.15 * it_o, (it_p, it_o)
     assert rel_err(xp, xo) < 1e-6
+
+
+@pytest.mark.parametrize("n", [8, 12, 16, 24])
+def test_cg_mixed_precision_small(gpu, n):
+    """Small elasticity systems converge fast; the FP32 correction must not
+    carry the whole solution (true FP64 residual checked independently)."""
+    mp, b = build(gpu, "elasticity", n=n)
+    x, it, res, st = solve(mp, b, api.ITER_CG, api.PREC_DIAG, tol=1e-8, precision=1)
+    assert st == 0 and res < 1e-8
+    r = b - mp.matvec(x)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.01e-8
 
 
 def test_cg_mixed_precision(gpu, oracle):
