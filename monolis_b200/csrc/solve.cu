@@ -173,25 +173,12 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // CG kernels
 // ---------------------------------------------------------------------------
-template <class T>
-struct Vec16;
-template <>
-struct Vec16<float> {
-  using type = float4;
-  static constexpr int n = 4;
-};
-template <>
-struct Vec16<double> {
-  using type = double2;
-  static constexpr int n = 2;
-};
-
 // P = beta*P + 1.0*Z (src/iterative/CG.f90:78-83); P = Z on iteration 1.
 // 16-byte vector accesses (work vectors are allocation-aligned), scalar tail.
 template <class T>
 __global__ void cg_p_kernel(long long n, T* __restrict__ p, const T* __restrict__ z, const SolverState* st) {
-  using V = typename Vec16<T>::type;
-  constexpr int W = Vec16<T>::n;
+  using V = typename Vec16T<T>::type;
+  constexpr int W = Vec16T<T>::n;
   if (st->done) return;
   const bool first = st->iter == 1;
   const T beta = (T)st->beta;
@@ -238,67 +225,83 @@ __global__ void __launch_bounds__(kThreads)
 // X = alpha*P + X; R = -alpha*Q + R; Z = M^-1 R; <R,R>, <R,Z>
 // (CG.f90:89-97 + the next iteration's precond apply and rho).
 // On iterations with iter % iter_RR == 0 only X is updated here and the
-// residual kernel recomputes R = B - A X. Blocks walk tiles of kThreads rows;
-// for B <= 3 a tile's vector segments are staged through shared memory.
+// residual kernel recomputes R = B - A X. Each thread owns R consecutive rows
+// (RowGroup) and moves them with 16-byte accesses; rows past the last full
+// group, or all rows when x is not 16-byte aligned, take the per-row path.
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     cg_update_kernel(int N, T* __restrict__ x, const T* __restrict__ p, T* __restrict__ r,
                      const T* __restrict__ q, T* __restrict__ z, const T* __restrict__ alu, int prec,
                      double* partials, unsigned int* ticket, SolverState* st, double* hist) {
-  constexpr bool kStage = B <= 3;
-  constexpr int kS = kStage ? kThreads * B : 1;
-  __shared__ T sx[kS], sp[kS], sr[kS], sq[kS];
+  using RG = RowGroup<T, B>;
+  constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
   const bool rr_iter = (st->iter % st->iter_rr) == 0;
   const T alpha = (T)st->alpha;
+  const bool alu_vec = (N % R) == 0;
+  const long long ngroups = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) ? N / R : 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
   double v[2] = {0.0, 0.0};
-  const int ntiles = (N + kThreads - 1) / kThreads;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long row0 = (long long)tile * kThreads;
-    const int nrows = (int)min((long long)kThreads, N - row0);
-    const int row = (int)row0 + threadIdx.x;
-    if (kStage) {
-      stage_in<T, B>(sx, x, row0, nrows);
-      stage_in<T, B>(sp, p, row0, nrows);
-      if (!rr_iter) {
-        stage_in<T, B>(sr, r, row0, nrows);
-        stage_in<T, B>(sq, q, row0, nrows);
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x < nrows) {
-      T t[B];
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
+    const long long row0 = g * R, e0 = row0 * B;
+    T xv[E], pv[E];
+    vload<T, E>(x + e0, xv);
+    vload<T, E>(p + e0, pv);
 #pragma unroll
-      for (int c = 0; c < B; c++) {
-        const int ls = threadIdx.x * B + c;
-        const long long i = (long long)row * B + c;
-        const T xv = axpy_rn(alpha, kStage ? sp[ls] : p[i], kStage ? sx[ls] : x[i]);
-        if (kStage) sx[ls] = xv; else x[i] = xv;
-        if (!rr_iter) t[c] = axpy_rn(-alpha, kStage ? sq[ls] : q[i], kStage ? sr[ls] : r[i]);
-      }
-      if (!rr_iter) {
-        T w[B];
+    for (int i = 0; i < E; i++) xv[i] = axpy_rn(alpha, pv[i], xv[i]);
+    vstore<T, E>(x + e0, xv);
+    if (!rr_iter) {
+      T rv[E], qv[E], zv[E];
+      vload<T, E>(r + e0, rv);
+      vload<T, E>(q + e0, qv);
 #pragma unroll
-        for (int c = 0; c < B; c++) w[c] = t[c];
-        if (prec) diag_row<B, T>(alu, N, row, w);
+      for (int i = 0; i < E; i++) rv[i] = axpy_rn(-alpha, qv[i], rv[i]);
 #pragma unroll
-        for (int c = 0; c < B; c++) {
-          const int ls = threadIdx.x * B + c;
-          const long long i = (long long)row * B + c;
-          if (kStage) { sr[ls] = t[c]; sq[ls] = w[c]; } else { r[i] = t[c]; z[i] = w[c]; }
-          v[0] += (double)t[c] * (double)t[c];
-          v[1] += (double)t[c] * (double)w[c];
+      for (int i = 0; i < E; i++) zv[i] = rv[i];
+      if (prec) {
+        T L[B * B][R];
+        load_alu_rows<T, B, R>(alu, N, row0, alu_vec, L);
+#pragma unroll
+        for (int k = 0; k < R; k++) {
+          T t[B];
+#pragma unroll
+          for (int c = 0; c < B; c++) t[c] = rv[k * B + c];
+          diag_solve<B, T>([&](int j, int kk) { return L[j * B + kk][k]; }, t);
+#pragma unroll
+          for (int c = 0; c < B; c++) zv[k * B + c] = t[c];
         }
       }
-    }
-    if (kStage) {
-      __syncthreads();
-      stage_out<T, B>(x, sx, row0, nrows);
-      if (!rr_iter) {
-        stage_out<T, B>(r, sr, row0, nrows);
-        stage_out<T, B>(z, sq, row0, nrows);
+#pragma unroll
+      for (int i = 0; i < E; i++) {
+        v[0] += (double)rv[i] * (double)rv[i];
+        v[1] += (double)rv[i] * (double)zv[i];
       }
-      __syncthreads();
+      vstore<T, E>(r + e0, rv);
+      vstore<T, E>(z + e0, zv);
+    }
+  }
+  for (long long row = ngroups * R + blockIdx.x * (long long)blockDim.x + threadIdx.x; row < N; row += stride) {
+    T t[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = row * B + c;
+      x[i] = axpy_rn(alpha, p[i], x[i]);
+      if (!rr_iter) {
+        t[c] = axpy_rn(-alpha, q[i], r[i]);
+        r[i] = t[c];
+      }
+    }
+    if (!rr_iter) {
+      T w[B];
+#pragma unroll
+      for (int c = 0; c < B; c++) w[c] = t[c];
+      if (prec) diag_row<B, T>(alu, N, (int)row, w);
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        z[row * B + c] = w[c];
+        v[0] += (double)t[c] * (double)t[c];
+        v[1] += (double)t[c] * (double)w[c];
+      }
     }
   }
   if (rr_iter) {
@@ -593,57 +596,73 @@ __global__ void __launch_bounds__(kThreads)
   });
 }
 
-// y += alpha*p; r -= alpha*q; z = M^-1 r; dots (FP32 vectors, FP64 sums)
+// y += alpha*p; r -= alpha*q; z = M^-1 r; dots (FP32 vectors, FP64 sums).
+// Register-blocked like cg_update_kernel (all vectors are the solver's own,
+// allocation-aligned).
 template <int B>
 __global__ void __launch_bounds__(kThreads)
     mixed_update_kernel(int N, float* __restrict__ y, const float* __restrict__ p, float* __restrict__ r,
                         const float* __restrict__ q, float* __restrict__ z, const float* __restrict__ alu, int prec,
                         double* partials, unsigned int* ticket, SolverState* st, double* hist) {
-  constexpr bool kStage = B <= 3;
-  constexpr int kS = kStage ? kThreads * B : 1;
-  __shared__ float sy[kS], sp[kS], sr[kS], sq[kS];
+  using RG = RowGroup<float, B>;
+  constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
   const float alpha = (float)st->alpha;
+  const bool alu_vec = (N % R) == 0;
+  const long long ngroups = N / R;
+  const long long stride = (long long)gridDim.x * blockDim.x;
   double v[2] = {0.0, 0.0};
-  const int ntiles = (N + kThreads - 1) / kThreads;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long long row0 = (long long)tile * kThreads;
-    const int nrows = (int)min((long long)kThreads, N - row0);
-    const int row = (int)row0 + threadIdx.x;
-    if (kStage) {
-      stage_in<float, B>(sy, y, row0, nrows);
-      stage_in<float, B>(sp, p, row0, nrows);
-      stage_in<float, B>(sr, r, row0, nrows);
-      stage_in<float, B>(sq, q, row0, nrows);
-      __syncthreads();
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
+    const long long row0 = g * R, e0 = row0 * B;
+    float yv[E], pv[E], rv[E], qv[E], zv[E];
+    vload<float, E>(y + e0, yv);
+    vload<float, E>(p + e0, pv);
+    vload<float, E>(r + e0, rv);
+    vload<float, E>(q + e0, qv);
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+      yv[i] = fmaf(alpha, pv[i], yv[i]);
+      rv[i] = fmaf(-alpha, qv[i], rv[i]);
+      zv[i] = rv[i];
     }
-    if (threadIdx.x < nrows) {
-      float t[B], w[B];
+    if (prec) {
+      float L[B * B][R];
+      load_alu_rows<float, B, R>(alu, N, row0, alu_vec, L);
 #pragma unroll
-      for (int c = 0; c < B; c++) {
-        const int ls = threadIdx.x * B + c;
-        const long long i = (long long)row * B + c;
-        const float yv = fmaf(alpha, kStage ? sp[ls] : p[i], kStage ? sy[ls] : y[i]);
-        if (kStage) sy[ls] = yv; else y[i] = yv;
-        t[c] = fmaf(-alpha, kStage ? sq[ls] : q[i], kStage ? sr[ls] : r[i]);
-        w[c] = t[c];
-      }
-      if (prec) diag_row<B, float>(alu, N, row, w);
+      for (int k = 0; k < R; k++) {
+        float t[B];
 #pragma unroll
-      for (int c = 0; c < B; c++) {
-        const int ls = threadIdx.x * B + c;
-        const long long i = (long long)row * B + c;
-        if (kStage) { sr[ls] = t[c]; sq[ls] = w[c]; } else { r[i] = t[c]; z[i] = w[c]; }
-        v[0] += (double)t[c] * (double)t[c];
-        v[1] += (double)t[c] * (double)w[c];
+        for (int c = 0; c < B; c++) t[c] = rv[k * B + c];
+        diag_solve<B, float>([&](int j, int kk) { return L[j * B + kk][k]; }, t);
+#pragma unroll
+        for (int c = 0; c < B; c++) zv[k * B + c] = t[c];
       }
     }
-    if (kStage) {
-      __syncthreads();
-      stage_out<float, B>(y, sy, row0, nrows);
-      stage_out<float, B>(r, sr, row0, nrows);
-      stage_out<float, B>(z, sq, row0, nrows);
-      __syncthreads();
+#pragma unroll
+    for (int i = 0; i < E; i++) {
+      v[0] += (double)rv[i] * (double)rv[i];
+      v[1] += (double)rv[i] * (double)zv[i];
+    }
+    vstore<float, E>(y + e0, yv);
+    vstore<float, E>(r + e0, rv);
+    vstore<float, E>(z + e0, zv);
+  }
+  for (long long row = ngroups * R + blockIdx.x * (long long)blockDim.x + threadIdx.x; row < N; row += stride) {
+    float t[B], w[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = row * B + c;
+      y[i] = fmaf(alpha, p[i], y[i]);
+      t[c] = fmaf(-alpha, q[i], r[i]);
+      r[i] = t[c];
+      w[c] = t[c];
+    }
+    if (prec) diag_row<B, float>(alu, N, (int)row, w);
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      z[row * B + c] = w[c];
+      v[0] += (double)t[c] * (double)t[c];
+      v[1] += (double)t[c] * (double)w[c];
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_mixed_inner(st, tot[0], tot[1], hist); });

@@ -171,12 +171,64 @@ __device__ __forceinline__ void stage_out(T* __restrict__ g, const T* s, long lo
   for (int i = threadIdx.x; i < len; i += blockDim.x) g[base + i] = s[i];
 }
 
-// z = M^-1 v for one block row with the in-place LU factors of the diagonal
-// block (entry-major: alu[e*N + row]); order of src/prec/diag/diag_nn.f90:
-// 195-229, which for B = 3 is the unrolled sequence of diag_33.f90:121-131.
-template <int B, class T>
-__device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int row, T (&t)[B]) {
-  auto L = [&](int j, int k) { return alu[(long long)(j * B + k) * N + row]; };
+// 16-byte vector type of an element type.
+template <class T>
+struct Vec16T;
+template <>
+struct Vec16T<float> {
+  using type = float4;
+  static constexpr int n = 4;
+};
+template <>
+struct Vec16T<double> {
+  using type = double2;
+  static constexpr int n = 2;
+};
+
+constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+
+// Register blocking of an interleaved vector x[row*B + c]: a thread owns R
+// consecutive block rows, E = R*B elements, a whole number of 16-byte words
+// (R = W / gcd(B, W) with W elements per word), so it moves them with E/W
+// aligned vector accesses.
+template <class T, int B>
+struct RowGroup {
+  static constexpr int W = Vec16T<T>::n;
+  static constexpr int R = W / gcd_c(B, W);
+  static constexpr int E = R * B;
+};
+
+template <class T, int E>
+__device__ __forceinline__ void vload(const T* __restrict__ p, T (&v)[E]) {
+  using V = typename Vec16T<T>::type;
+  constexpr int W = Vec16T<T>::n;
+#pragma unroll
+  for (int i = 0; i < E / W; i++) {
+    const V t = reinterpret_cast<const V*>(p)[i];
+    const T* e = reinterpret_cast<const T*>(&t);
+#pragma unroll
+    for (int k = 0; k < W; k++) v[i * W + k] = e[k];
+  }
+}
+template <class T, int E>
+__device__ __forceinline__ void vstore(T* __restrict__ p, const T (&v)[E]) {
+  using V = typename Vec16T<T>::type;
+  constexpr int W = Vec16T<T>::n;
+#pragma unroll
+  for (int i = 0; i < E / W; i++) {
+    V t;
+    T* e = reinterpret_cast<T*>(&t);
+#pragma unroll
+    for (int k = 0; k < W; k++) e[k] = v[i * W + k];
+    reinterpret_cast<V*>(p)[i] = t;
+  }
+}
+
+// In-place LU solve of one B x B diagonal block with the factors in L
+// (row-major), order of src/prec/diag/diag_nn.f90:195-229 (for B = 3 the
+// unrolled sequence of diag_33.f90:121-131).
+template <int B, class T, class F>
+__device__ __forceinline__ void diag_solve(F L, T (&t)[B]) {
 #pragma unroll
   for (int j = 1; j < B; j++)
 #pragma unroll
@@ -187,6 +239,36 @@ __device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int r
     for (int k = B - 1; k > j; k--) t[j] = sub_rn(t[j], mul_rn(L(j, k), t[k]));
     t[j] = mul_rn(L(j, j), t[j]);
   }
+}
+
+// Factors of R consecutive rows, entry-major storage alu[e*N + row]: one
+// vector load per entry when R words fill 16 bytes and N keeps them aligned.
+template <class T, int B, int R>
+__device__ __forceinline__ void load_alu_rows(const T* __restrict__ alu, int N, long long row0, bool vec_ok,
+                                              T (&L)[B * B][R]) {
+#pragma unroll
+  for (int e = 0; e < B * B; e++) {
+    const T* src = alu + (long long)e * N + row0;
+    if constexpr (R * sizeof(T) == 16) {
+      if (vec_ok) {
+        T v[R];
+        vload<T, R>(src, v);
+#pragma unroll
+        for (int k = 0; k < R; k++) L[e][k] = v[k];
+        continue;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < R; k++) L[e][k] = src[k];
+  }
+}
+
+// z = M^-1 v for one block row with the in-place LU factors of the diagonal
+// block (entry-major: alu[e*N + row]); order of src/prec/diag/diag_nn.f90:
+// 195-229, which for B = 3 is the unrolled sequence of diag_33.f90:121-131.
+template <int B, class T>
+__device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int row, T (&t)[B]) {
+  diag_solve<B, T>([&](int j, int k) { return alu[(long long)(j * B + k) * N + row]; }, t);
 }
 
 }  // namespace mb
