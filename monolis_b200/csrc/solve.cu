@@ -23,6 +23,7 @@
 // update expressions and roundings, true residual every 200 iterations,
 // convergence relative to the initial residual); only the order in which the
 // dot products are summed differs (tree instead of serial).
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -66,6 +67,13 @@ int pgrid(K kernel) {
   cache[key] = g;
   return g;
 }
+
+// Grid of a matrix kernel: one thread per row (or row pair), up to the
+// capacity of the reduction scratch, beyond which the kernels grid-stride.
+// The hardware block scheduler balances the uneven slice widths better than
+// a fixed grid-stride assignment does.
+constexpr int kMaxGrid = 65536;
+inline int row_grid(long long rows) { return (int)std::min<long long>(blocks_for(rows), kMaxGrid); }
 
 // ---------------------------------------------------------------------------
 // Scalar updates run by the last block of a grid reduction.
@@ -872,13 +880,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       double* x = d_x;
       const double* b = d_b;
       auto k_resid = resid_kernel<B, U, double, double>;
-      const int g_resid = pgrid(k_resid);
+      const int g_resid = row_grid(N);
       if (p.method == 1) {
         double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n), *pp = vec.get<double>(n);
         if (!r || !z || !q || !pp) return kCudaError;
         auto k_spmv = cg_spmv_kernel<B, U, double, double>;
         auto k_upd = cg_update_kernel<B, double>;
-        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+        const int g_spmv = row_grid(N), g_upd = pgrid(k_upd);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
         plan.kernels = 4;
         plan.kind = {1, 0, 2, 0};
@@ -902,7 +910,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_v = bicg_v_kernel<B, U, double, double>;
         auto k_t = bicg_t_kernel<B, U, double, double>;
         auto k_xr = bicg_xr_kernel<B, double>;
-        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
+        const int g_v = row_grid(N), g_t = row_grid(N), g_xr = pgrid(k_xr);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
         plan.kernels = 6;
         plan.kind = {2, 0, 2, 0, 1, 0};
@@ -934,10 +942,10 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_spmv = cg_spmv2_kernel<B, U>;
       auto k_upd = mixed_update_kernel<B>;
       auto k_ref = mixed_refresh_kernel<B>;
-      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
-      const int g_ref = 2 * num_sms();  // mostly a no-op: small grid
+      const int g_spmv = row_grid((N + 1) / 2), g_upd = pgrid(k_upd);
+      const int g_ref = row_grid(N);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
-      k_ref<<<pgrid(k_ref), kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
+      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
       plan.kernels = 4;
       plan.always_all = true;
       plan.kind = {1, 0, 2, 0};
