@@ -101,6 +101,55 @@ int monolis_b200_device_matvec_R32(MONOLIS* mat, const float* d_x, float* d_y);
 /* Layout facts of the prepared device matrix (block counts). */
 int monolis_b200_device_info(MONOLIS* mat, long long* nz_blocks, long long* padded_blocks, int* n_slices);
 
+/* ---- adjoint (transpose solve, sampled outer product, element gradients) ----
+ * No counterpart in the reference library, which has no transpose product
+ * or gradient. They let a caller differentiate a loss L(x) of the solution
+ * of A(k) x = b with A = sum_e k_e K_e:
+ *   1. monolis_solve_R                      x
+ *   2. monolis_b200_solve_transpose_R       A^T lambda = dL/dx
+ *   3. monolis_b200_element_gradient_R      dL/dk_e = -lambda_e^T K_e x_e
+ * (or monolis_b200_sampled_outer_product_R for dL/dA over the pattern). */
+
+/* A^T x = b with the struct's method, preconditioner, tolerance and
+ * precision; same calling convention, parameters and outputs as
+ * monolis_solve_R. A^T is built on the device from the struct's CSC arrays
+ * (pattern + the CSC permutation of monolis_get_CSC_format) and cached with
+ * the device matrix. One rank (N == NP). */
+int monolis_b200_solve_transpose_R(MONOLIS* mat, MONOLIS_COM* com, double* b, double* x);
+int monolis_b200_device_solve_transpose_R(MONOLIS* mat, const double* d_b, double* d_x);
+
+/* y = A^T x (host vectors / device vectors). Row j of A^T sums the blocks of
+ * column j of A in ascending row order. */
+int monolis_b200_matvec_transpose_R(MONOLIS* mat, MONOLIS_COM* com, double* x, double* y);
+int monolis_b200_device_matvec_transpose_R(MONOLIS* mat, const double* d_x, double* d_y);
+
+/* G = scale * lambda x^T sampled on the sparsity pattern, in the layout of
+ * mat->mat.R.A (NZ blocks of ndof^2 values, row-major in the block): entry
+ * (r,c) of stored block (i,j) is scale * lambda[i*ndof+r] * x[j*ndof+c].
+ * With scale = -1 and A lambda-adjoint as above, G = dL/dA. */
+int monolis_b200_sampled_outer_product_R(MONOLIS* mat, const double* lambda, const double* x, double scale,
+                                         double* G);
+int monolis_b200_device_sampled_outer_product_R(MONOLIS* mat, const double* d_lambda, const double* d_x,
+                                                double scale, double* d_G);
+
+/* Per-element reduction of the sampled outer product:
+ *   grad[e] = scale * sum_{a,b} lambda_a K_e(a,b) x_b
+ * over the n_base*ndof local dofs of element e (elem[e*n_base + q], 0-based
+ * nodes; local dof a = q*ndof + d, the order of the element matrices of
+ * monolis_add_matrix_to_sparse_matrix_R). K_e is Ke + e*ke_stride (row-major,
+ * (n_base*ndof)^2 values); ke_stride 0 shares one matrix. Rows of dofs with
+ * fixed_dof[dof] != 0 are skipped (the Dirichlet rows that
+ * monolis_set_Dirichlet_bc_R replaced do not depend on k); fixed_dof may be
+ * NULL. With scale = -1 this is dL/dk_e. The host form checks the node ids;
+ * the device form requires 0 <= elem < NP. */
+int monolis_b200_element_gradient_R(MONOLIS* mat, int n_elem, int n_base, const int* elem, const double* Ke,
+                                    long long ke_stride, const double* lambda, const double* x,
+                                    const int* fixed_dof, double scale, double* grad);
+int monolis_b200_device_element_gradient_R(MONOLIS* mat, int n_elem, int n_base, const int* d_elem,
+                                           const double* d_Ke, long long ke_stride, const double* d_lambda,
+                                           const double* d_x, const int* d_fixed_dof, double scale,
+                                           double* d_grad);
+
 /* ---- allocation-free inner product ----
  * No counterpart in the reference library.
  * *d_sum = sum_i d_x[i]*d_y[i] for device vectors of length n, enqueued on

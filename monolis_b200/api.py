@@ -156,6 +156,18 @@ _PRODUCT = {
                                            C.POINTER(C.c_int)]),
     "monolis_b200_inner_product_noalloc_R": (C.c_int, [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                                        C.c_void_p]),
+    "monolis_b200_solve_transpose_R": (C.c_int, [_MP, _CP, _dp, _dp]),
+    "monolis_b200_device_solve_transpose_R": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
+    "monolis_b200_matvec_transpose_R": (C.c_int, [_MP, _CP, _dp, _dp]),
+    "monolis_b200_device_matvec_transpose_R": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
+    "monolis_b200_sampled_outer_product_R": (C.c_int, [_MP, _dp, _dp, C.c_double, _dp]),
+    "monolis_b200_device_sampled_outer_product_R": (C.c_int, [_MP, C.c_void_p, C.c_void_p, C.c_double,
+                                                              C.c_void_p]),
+    "monolis_b200_element_gradient_R": (C.c_int, [_MP, C.c_int, C.c_int, _ip, _dp, C.c_longlong, _dp, _dp, _ip,
+                                                  C.c_double, _dp]),
+    "monolis_b200_device_element_gradient_R": (C.c_int, [_MP, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                         C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                         C.c_double, C.c_void_p]),
 }
 
 _ORACLE_EXTRA = {
@@ -417,6 +429,46 @@ class Monolis:
         b = np.ascontiguousarray(b)
         self.lib.monolis_solve_R(self.p, C.pointer(self.com), _dptr(b), _dptr(x))
         return x
+
+    # ---- adjoint pieces (product only) ----
+    def solve_transpose(self, b, x):
+        """monolis_b200_solve_transpose_R: A^T x = b, x updated in place."""
+        assert b.dtype == np.float64 and x.dtype == np.float64 and x.flags.c_contiguous
+        b = np.ascontiguousarray(b)
+        return self.lib.monolis_b200_solve_transpose_R(self.p, C.pointer(self.com), _dptr(b), _dptr(x))
+
+    def matvec_transpose(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros_like(x)
+        rc = self.lib.monolis_b200_matvec_transpose_R(self.p, C.pointer(self.com), _dptr(x), _dptr(y))
+        if rc:
+            raise RuntimeError(f"matvec_transpose failed: {STATUS_NAMES.get(rc, rc)}")
+        return y
+
+    def sampled_outer_product(self, lam, x, scale=-1.0):
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        nd = self.NDOF
+        G = np.empty(self.NZ * nd * nd)
+        rc = self.lib.monolis_b200_sampled_outer_product_R(self.p, _dptr(lam), _dptr(x), scale, _dptr(G))
+        if rc:
+            raise RuntimeError(f"sampled_outer_product failed: {STATUS_NAMES.get(rc, rc)}")
+        return G
+
+    def element_gradient(self, elem, n_base, Ke, ke_stride, lam, x, fixed=None, scale=-1.0):
+        elem = np.ascontiguousarray(elem, dtype=np.int32)
+        Ke = np.ascontiguousarray(Ke, dtype=np.float64)
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        n_elem = elem.size // n_base
+        grad = np.empty(n_elem)
+        fx = None if fixed is None else np.ascontiguousarray(fixed, dtype=np.int32)
+        rc = self.lib.monolis_b200_element_gradient_R(self.p, n_elem, n_base, _iptr(elem), _dptr(Ke), ke_stride,
+                                                      _dptr(lam), _dptr(x), None if fx is None else _iptr(fx),
+                                                      scale, _dptr(grad))
+        if rc:
+            raise RuntimeError(f"element_gradient failed: {STATUS_NAMES.get(rc, rc)}")
+        return grad
 
     # ---- device entry points (product only) ----
     def device_prepare(self):

@@ -31,6 +31,12 @@
 
 namespace {
 
+// Return MONOLIS_B200_CUDA_ERROR from an entry point when a CUDA call fails.
+#define MB_API_CUDA(call)                                   \
+  do {                                                      \
+    if ((call) != cudaSuccess) return MONOLIS_B200_CUDA_ERROR; \
+  } while (0)
+
 double now_sec() {
   using namespace std::chrono;
   return duration<double>(steady_clock::now().time_since_epoch()).count();
@@ -237,6 +243,8 @@ void add_element(MONOLIS_MAT* a, int n1, int n2, const int* e1, const int* e2, c
 // ---------------------------------------------------------------------------
 struct DevState {
   mb::SellMatrix A;
+  mb::SellMatrix AT;  // A^T, built on demand from A's device CSR and the CSC arrays
+  long long build_id = 0, at_build_id = -1;
   mb::Scratch sc;
   double* d_b = nullptr;
   double* d_x = nullptr;
@@ -296,6 +304,7 @@ void state_release(const MONOLIS* m) {
   if (c.init) {
     cudaStreamSynchronize(c.stream);
     mb::sell_free(s->A);
+    mb::sell_free(s->AT);
     mb::scratch_free(s->sc);
     cudaFree(s->d_b);
     cudaFree(s->d_x);
@@ -362,6 +371,7 @@ int prepare(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32, double* t_h
     s->key_ndof = a->NDOF;
     s->key_version = I[MONOLIS_B200_PRM_I_MATRIX_VERSION];
     s->prepared = true;
+    s->build_id++;
   }
   if (need_diag && !s->A.have_alu) {
     int rc = mb::diag_setup(s->A, st);
@@ -373,6 +383,45 @@ int prepare(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32, double* t_h
   }
   m->prm.Iarray[MONOLIS_B200_PRM_I_UNROLL_FP64] = s->A.u64;
   m->prm.Iarray[MONOLIS_B200_PRM_I_UNROLL_FP32] = s->A.have_val32 ? s->A.u32 : 0;
+  return mb::kOk;
+}
+
+// A^T of the prepared matrix (rebuilt whenever A was), with its DIAG factors
+// and FP32 copies as asked.
+int prepare_transpose(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32) {
+  MONOLIS_MAT* a = &m->mat;
+  if (a->N != a->NP) {
+    fprintf(stderr, "** monolis_b200: transpose needs N == NP (one rank)\n");
+    return mb::kBadInput;
+  }
+  cudaStream_t st = ctx().stream;
+  if (s->at_build_id != s->build_id) {
+    const int* ci = a->CSC.index;
+    const int* cit = a->CSC.item;
+    const int* cp = a->CSC.perm;
+    std::vector<int> bi, bit, bp;
+    if (!ci || !cit || !cp) {
+      const int nz = a->CSR.index[a->N];
+      bi.resize((size_t)a->N + 1);
+      bit.resize((size_t)nz);
+      bp.resize((size_t)nz);
+      monolis_get_CSC_format(a->N, a->NP, nz, a->CSR.index, a->CSR.item, bi.data(), bit.data(), bp.data());
+      ci = bi.data();
+      cit = bit.data();
+      cp = bp.data();
+    }
+    int rc = mb::sell_build_transpose(s->AT, s->A, ci, cit, cp, st);
+    if (rc) return rc;
+    s->at_build_id = s->build_id;
+  }
+  if (need_diag && !s->AT.have_alu) {
+    int rc = mb::diag_setup(s->AT, st);
+    if (rc) return rc;
+  }
+  if (need_fp32 && !s->AT.have_val32) {
+    int rc = mb::sell_make_fp32(s->AT, st);
+    if (rc) return rc;
+  }
   return mb::kOk;
 }
 
@@ -389,8 +438,8 @@ const char* str_prec(int p) {
 
 // Solve with device b/x already resident; prints and fills prm like
 // src/solver/solver.f90:77-185 + src/define/def_solver_prm.f90:255-355.
-int solve_resident(MONOLIS* m, DevState* s, const double* d_b, double* d_x, double t_start, double t_prep,
-                   double t_h2d) {
+int solve_resident(MONOLIS* m, DevState* s, mb::SellMatrix& A, const double* d_b, double* d_x, double t_start,
+                   double t_prep, double t_h2d) {
   int* I = m->prm.Iarray;
   double* R = m->prm.Rarray;
   mb::SolveParams p{};
@@ -412,7 +461,7 @@ int solve_resident(MONOLIS* m, DevState* s, const double* d_b, double* d_x, doub
   std::vector<double> hist;
   if (log) hist.assign((size_t)std::max(p.max_iter, 0) + 2, 0.0);
   mb::SolveResult res;
-  int rc = mb::solve_device(s->A, s->sc, p, d_b, d_x, res, log ? hist.data() : nullptr, ctx().stream);
+  int rc = mb::solve_device(A, s->sc, p, d_b, d_x, res, log ? hist.data() : nullptr, ctx().stream);
   if (rc) {
     I[MONOLIS_PRM_I_IERR] = rc;
     return rc;
@@ -822,33 +871,38 @@ void monolis_inner_product_R(MONOLIS* m, MONOLIS_COM* com, int n_dof, double* x,
   if (cudaStreamSynchronize(st) != cudaSuccess) error_stop("monolis_inner_product_R: CUDA error");
 }
 
-// src/solver/solver.f90:29-49 + wrapper/solver/monolis_solver_c.c:8-60
-void monolis_solve_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) {
+}  // extern "C"
+
+// src/solver/solver.f90:29-49 + wrapper/solver/monolis_solver_c.c:8-60, for A
+// or (transpose) A^T.
+static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool transpose) {
   const double t_start = now_sec();
   int* I = m->prm.Iarray;
   if (com && com->comm_size > 1) {
     fprintf(stderr, "** monolis_b200: one rank per solve in this library (comm_size=%d)\n", com->comm_size);
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
-    return;
+    return MONOLIS_B200_BAD_INPUT;
   }
   if (!method_supported(m)) {
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
-    return;
+    return MONOLIS_B200_BAD_INPUT;
   }
   std::lock_guard<std::mutex> lk(g_ctx_mu);
   if (ctx_init()) {
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_CUDA_ERROR;
-    return;
+    return MONOLIS_B200_CUDA_ERROR;
   }
   DevState* s = state_of(m);
   const bool mixed = I[MONOLIS_B200_PRM_I_PRECISION] == 1;
   double t_h2d = 0.0;
-  int rc = prepare(m, s, I[MONOLIS_PRM_I_PRECOND] == MONOLIS_PREC_DIAG, mixed, &t_h2d);
+  const bool diag = I[MONOLIS_PRM_I_PRECOND] == MONOLIS_PREC_DIAG;
+  int rc = prepare(m, s, diag && !transpose, mixed && !transpose, &t_h2d);
+  if (!rc && transpose) rc = prepare_transpose(m, s, diag, mixed);
   const size_t n = (size_t)m->mat.N * m->mat.NDOF;
   if (!rc) rc = ensure_vec(s, n);
   if (rc) {
     I[MONOLIS_PRM_I_IERR] = rc;
-    return;
+    return rc;
   }
   cudaStream_t st = ctx().stream;
   // B and X are copied into the struct's own arrays first, as the reference
@@ -861,12 +915,12 @@ void monolis_solve_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) {
     cudaMemcpyAsync(s->d_x, x, n * sizeof(double), cudaMemcpyHostToDevice, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) {
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_CUDA_ERROR;
-    return;
+    return MONOLIS_B200_CUDA_ERROR;
   }
   t_h2d += now_sec() - t1;
   const double t_prep = now_sec() - t_start;
-  rc = solve_resident(m, s, s->d_b, s->d_x, t_start, t_prep, t_h2d);
-  if (rc) return;
+  rc = solve_resident(m, s, transpose ? s->AT : s->A, s->d_b, s->d_x, t_start, t_prep, t_h2d);
+  if (rc) return rc;
   const double t2 = now_sec();
   cudaMemcpyAsync(x, s->d_x, n * sizeof(double), cudaMemcpyDeviceToHost, st);
   cudaStreamSynchronize(st);
@@ -877,7 +931,17 @@ void monolis_solve_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) {
   if (I[MONOLIS_PRM_I_IERR] == MONOLIS_B200_MAXITER && I[MONOLIS_PRM_I_IS_MEASUREMENT] == MONOLIS_I_FALSE &&
       I[MONOLIS_PRM_I_IS_ERROR_ABORT] == MONOLIS_I_TRUE)
     error_stop("reached the maximum number of iterations");  // src/linalg/mat_converge.f90:134-140
+  return I[MONOLIS_PRM_I_IERR];
 }
+
+extern "C" {
+
+void monolis_solve_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) { solve_host(m, com, b, x, false); }
+
+int monolis_b200_solve_transpose_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) {
+  return solve_host(m, com, b, x, true);
+}
+
 
 // ---- monolis_b200 extensions ----
 int monolis_b200_set_precision(MONOLIS* m, int precision) {
@@ -922,10 +986,141 @@ int monolis_b200_device_solve_R(MONOLIS* m, const double* d_b, double* d_x) {
     int rc = mb::diag_setup(s->A, ctx().stream);
     if (rc) return rc;
   }
-  int rc = solve_resident(m, s, d_b, d_x, t_start, 0.0, 0.0);
+  int rc = solve_resident(m, s, s->A, d_b, d_x, t_start, 0.0, 0.0);
   if (rc) return rc;
   print_summary(m);
   return m->prm.Iarray[MONOLIS_PRM_I_IERR];
+}
+
+int monolis_b200_device_solve_transpose_R(MONOLIS* m, const double* d_b, double* d_x) {
+  const double t_start = now_sec();
+  if (!method_supported(m)) return MONOLIS_B200_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared) return MONOLIS_B200_BAD_INPUT;
+  const int* I = m->prm.Iarray;
+  int rc = prepare_transpose(m, s, I[MONOLIS_PRM_I_PRECOND] == MONOLIS_PREC_DIAG,
+                             I[MONOLIS_B200_PRM_I_PRECISION] == 1);
+  if (rc) return rc;
+  rc = solve_resident(m, s, s->AT, d_b, d_x, t_start, 0.0, 0.0);
+  if (rc) return rc;
+  print_summary(m);
+  return m->prm.Iarray[MONOLIS_PRM_I_IERR];
+}
+
+int monolis_b200_device_matvec_transpose_R(MONOLIS* m, const double* d_x, double* d_y) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared) return MONOLIS_B200_BAD_INPUT;
+  int rc = prepare_transpose(m, s, false, false);
+  if (rc) return rc;
+  return mb::spmv64(s->AT, d_x, d_y, ctx().stream);
+}
+
+int monolis_b200_matvec_transpose_R(MONOLIS* m, MONOLIS_COM* com, double* x, double* y) {
+  if (com && com->comm_size > 1) return MONOLIS_B200_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  int rc = prepare(m, s, false, false, nullptr);
+  if (!rc) rc = prepare_transpose(m, s, false, false);
+  const size_t n = (size_t)m->mat.N * m->mat.NDOF;
+  if (!rc) rc = ensure_vec(s, n);
+  if (rc) return rc;
+  cudaStream_t st = ctx().stream;
+  MB_API_CUDA(cudaMemcpyAsync(s->d_x, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  rc = mb::spmv64(s->AT, s->d_x, s->d_y, st);
+  if (rc) return rc;
+  MB_API_CUDA(cudaMemcpyAsync(y, s->d_y, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  MB_API_CUDA(cudaStreamSynchronize(st));
+  return MONOLIS_B200_OK;
+}
+
+int monolis_b200_device_sampled_outer_product_R(MONOLIS* m, const double* d_lambda, const double* d_x, double scale,
+                                                double* d_G) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared) return MONOLIS_B200_BAD_INPUT;
+  return mb::outer_product64(s->A, d_lambda, d_x, scale, d_G, ctx().stream);
+}
+
+int monolis_b200_sampled_outer_product_R(MONOLIS* m, const double* lambda, const double* x, double scale,
+                                         double* G) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  int rc = prepare(m, s, false, false, nullptr);
+  const size_t n = (size_t)m->mat.N * m->mat.NDOF;
+  if (!rc) rc = ensure_vec(s, n);
+  if (rc) return rc;
+  cudaStream_t st = ctx().stream;
+  const size_t ng = (size_t)s->A.nz * m->mat.NDOF * m->mat.NDOF;
+  double* d_G = nullptr;
+  MB_API_CUDA(cudaMallocAsync((void**)&d_G, ng * sizeof(double) + 16, st));
+  MB_API_CUDA(cudaMemcpyAsync(s->d_x, x, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  MB_API_CUDA(cudaMemcpyAsync(s->d_y, lambda, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  rc = mb::outer_product64(s->A, s->d_y, s->d_x, scale, d_G, st);
+  if (!rc && cudaMemcpyAsync(G, d_G, ng * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    rc = MONOLIS_B200_CUDA_ERROR;
+  cudaFreeAsync(d_G, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc = MONOLIS_B200_CUDA_ERROR;
+  return rc;
+}
+
+int monolis_b200_device_element_gradient_R(MONOLIS* m, int n_elem, int n_base, const int* d_elem, const double* d_Ke,
+                                           long long ke_stride, const double* d_lambda, const double* d_x,
+                                           const int* d_fixed_dof, double scale, double* d_grad) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  return mb::element_gradient64(n_elem, n_base, m->mat.NDOF, d_elem, d_Ke, ke_stride, d_lambda, d_x, d_fixed_dof,
+                                scale, d_grad, ctx().stream);
+}
+
+int monolis_b200_element_gradient_R(MONOLIS* m, int n_elem, int n_base, const int* elem, const double* Ke,
+                                    long long ke_stride, const double* lambda, const double* x,
+                                    const int* fixed_dof, double scale, double* grad) {
+  const MONOLIS_MAT* a = &m->mat;
+  if (n_elem < 0 || n_base <= 0 || ke_stride < 0 || a->NDOF <= 0) return MONOLIS_B200_BAD_INPUT;
+  for (long long k = 0; k < (long long)n_elem * n_base; k++)
+    if (elem[k] < 0 || elem[k] >= a->NP) return MONOLIS_B200_BAD_INPUT;
+  if (n_elem == 0) return MONOLIS_B200_OK;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  cudaStream_t st = ctx().stream;
+  const long long nl = (long long)n_base * a->NDOF;
+  const size_t n = (size_t)a->NP * a->NDOF;
+  const size_t nk = ke_stride == 0 ? (size_t)(nl * nl) : (size_t)(ke_stride * (n_elem - 1) + nl * nl);
+  const size_t ne = (size_t)n_elem * n_base;
+  // one device buffer: elem | fixed | Ke | lambda | x | grad, 16-byte aligned parts
+  auto al = [](size_t b) { return (b + 15) / 16 * 16; };
+  const size_t o_fix = al(ne * sizeof(int)), o_ke = o_fix + al(fixed_dof ? n * sizeof(int) : 0);
+  const size_t o_l = o_ke + al(nk * sizeof(double)), o_x = o_l + al(n * sizeof(double));
+  const size_t o_g = o_x + al(n * sizeof(double)), total = o_g + al((size_t)n_elem * sizeof(double));
+  char* buf = nullptr;
+  MB_API_CUDA(cudaMallocAsync((void**)&buf, total, st));
+  int rc = MONOLIS_B200_OK;
+  auto up = [&](size_t off, const void* src, size_t bytes) {
+    if (!rc && bytes && cudaMemcpyAsync(buf + off, src, bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      rc = MONOLIS_B200_CUDA_ERROR;
+  };
+  up(0, elem, ne * sizeof(int));
+  if (fixed_dof) up(o_fix, fixed_dof, n * sizeof(int));
+  up(o_ke, Ke, nk * sizeof(double));
+  up(o_l, lambda, n * sizeof(double));
+  up(o_x, x, n * sizeof(double));
+  if (!rc)
+    rc = mb::element_gradient64(n_elem, n_base, a->NDOF, (const int*)buf, (const double*)(buf + o_ke), ke_stride,
+                                (const double*)(buf + o_l), (const double*)(buf + o_x),
+                                fixed_dof ? (const int*)(buf + o_fix) : nullptr, scale, (double*)(buf + o_g), st);
+  if (!rc && cudaMemcpyAsync(grad, buf + o_g, (size_t)n_elem * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+                 cudaSuccess)
+    rc = MONOLIS_B200_CUDA_ERROR;
+  cudaFreeAsync(buf, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc = MONOLIS_B200_CUDA_ERROR;
+  return rc;
 }
 
 int monolis_b200_device_matvec_R(MONOLIS* m, const double* d_x, double* d_y) {

@@ -88,6 +88,12 @@ struct Scratch {
 // ---- matrix build on the device ----
 int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const double* h_val,
                int N, int ndof, cudaStream_t s, double* t_h2d);
+// Slices and FP64 values from the device CSR (d_rowptr, d_item, d_csrval).
+int sell_layout(SellMatrix& m, cudaStream_t s);
+// A^T from A's device CSR and the host CSC arrays of the pattern (offsets,
+// 1-based rows, 1-based CSR positions; monolis_get_CSC_format).
+int sell_build_transpose(SellMatrix& at, const SellMatrix& a, const int* h_csc_index, const int* h_csc_item,
+                         const int* h_csc_perm, cudaStream_t s);
 int sell_make_fp32(SellMatrix& m, cudaStream_t s);
 // Times the SpMV unroll variants on the matrix and keeps the fastest (u64 / u32).
 int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s);
@@ -99,6 +105,17 @@ int spmv64(const SellMatrix& m, const double* x, double* y, cudaStream_t s);
 int spmv32(const SellMatrix& m, const float* x, float* y, cudaStream_t s);
 int dot64(long long n, const double* x, const double* y, double* out, Scratch& sc, cudaStream_t s);
 int diag_apply64(const SellMatrix& m, const double* x, double* y, cudaStream_t s);
+
+// ---- adjoint pieces (adjoint.cu) ----
+// G (stored blocks x ndof^2, the layout of the matrix values) =
+// scale * lambda_i x_j^T over the pattern of m.
+int outer_product64(const SellMatrix& m, const double* lam, const double* x, double scale, double* G,
+                    cudaStream_t s);
+// grad[e] = scale * sum_ab lam_a K_e(a,b) x_b over each element's local dofs,
+// lam_a taken as zero where fixed[dof] != 0 (fixed may be null).
+int element_gradient64(int n_elem, int n_base, int ndof, const int* elem, const double* Ke, long long ke_stride,
+                       const double* lam, const double* x, const int* fixed, double scale, double* grad,
+                       cudaStream_t s);
 
 // ---- solvers (device-resident loops) ----
 struct SolveParams {

@@ -192,20 +192,6 @@ __global__ void diag_apply_kernel(const double* __restrict__ alu, int N, const d
   for (int b = 0; b < B; b++) y[(long long)i * B + b] = t[b];
 }
 
-template <class F>
-int dispatch_ndof(int ndof, F&& f) {
-  switch (ndof) {
-    case 1: return f(std::integral_constant<int, 1>{});
-    case 2: return f(std::integral_constant<int, 2>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    case 4: return f(std::integral_constant<int, 4>{});
-    case 5: return f(std::integral_constant<int, 5>{});
-    case 6: return f(std::integral_constant<int, 6>{});
-    default:
-      fprintf(stderr, "** monolis_b200: NDOF=%d is not supported on the device (1..6)\n", ndof);
-      return kBadInput;
-  }
-}
 
 }  // namespace
 
@@ -214,17 +200,12 @@ int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const doubl
   if (N <= 0 || ndof <= 0) return kBadInput;
   const long long nz = h_index[N];
   const int B2 = ndof * ndof;
-  const int nslices = (N + kSlice - 1) / kSlice;
   m.N = N;
   m.ndof = ndof;
   m.nz = nz;
-  m.nslices = nslices;
-  m.have_val32 = m.have_alu = m.have_alu32 = false;
   MB_CUDA_OK(grow(&m.d_rowptr, m.cap_rowptr, (size_t)N + 1));
-  MB_CUDA_OK(grow(&m.d_slptr, m.cap_slptr, (size_t)nslices + 1));
   MB_CUDA_OK(grow(&m.d_item, m.cap_item, (size_t)nz));
   MB_CUDA_OK(grow(&m.d_csrval, m.cap_csrval, (size_t)nz * B2));
-
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -233,7 +214,24 @@ int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const doubl
   MB_CUDA_OK(cudaMemcpyAsync(m.d_item, h_item, sizeof(int) * nz, cudaMemcpyHostToDevice, s));
   MB_CUDA_OK(cudaMemcpyAsync(m.d_csrval, h_val, sizeof(double) * nz * B2, cudaMemcpyHostToDevice, s));
   cudaEventRecord(e1, s);
+  int rc = sell_layout(m, s);
+  if (t_h2d) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);  // sell_layout has synchronized the stream
+    *t_h2d = ms * 1e-3;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
 
+int sell_layout(SellMatrix& m, cudaStream_t s) {
+  const int N = m.N, ndof = m.ndof;
+  const int B2 = ndof * ndof;
+  const int nslices = (N + kSlice - 1) / kSlice;
+  m.nslices = nslices;
+  m.have_val32 = m.have_alu = m.have_alu32 = false;
+  MB_CUDA_OK(grow(&m.d_slptr, m.cap_slptr, (size_t)nslices + 1));
   // slice widths -> prefix on the host (nslices = N/32 values) -> slice pointers
   long long* d_w = nullptr;
   MB_CUDA_OK(cudaMallocAsync((void**)&d_w, sizeof(long long) * nslices, s));
@@ -242,13 +240,6 @@ int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const doubl
   MB_CUDA_OK(cudaMemcpyAsync(w.data(), d_w, sizeof(long long) * nslices, cudaMemcpyDeviceToHost, s));
   MB_CUDA_OK(cudaStreamSynchronize(s));
   cudaFreeAsync(d_w, s);
-  if (t_h2d) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    *t_h2d = ms * 1e-3;
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   ptr[0] = 0;
   for (int i = 0; i < nslices; i++) ptr[i + 1] = ptr[i] + w[i];
   m.padded = ptr[nslices];
@@ -342,14 +333,6 @@ void sell_free(SellMatrix& m) {
   m = SellMatrix();
 }
 
-template <class F>
-int dispatch_u(int u, F&& f) {
-  switch (u) {
-    case 1: return f(std::integral_constant<int, 1>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    default: return f(std::integral_constant<int, 2>{});
-  }
-}
 
 int spmv64_u(const SellMatrix& m, int u, const double* x, double* y, cudaStream_t s) {
   SellView<double> A = view_of<double>(m);

@@ -764,27 +764,7 @@ __global__ void mixed_fold_kernel(long long n, double* __restrict__ x, float* __
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-template <class F>
-int dispatch_ndof(int ndof, F&& f) {
-  switch (ndof) {
-    case 1: return f(std::integral_constant<int, 1>{});
-    case 2: return f(std::integral_constant<int, 2>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    case 4: return f(std::integral_constant<int, 4>{});
-    case 5: return f(std::integral_constant<int, 5>{});
-    case 6: return f(std::integral_constant<int, 6>{});
-    default: return kBadInput;
-  }
-}
 
-template <class F>
-int dispatch_u(int u, F&& f) {
-  switch (u) {
-    case 1: return f(std::integral_constant<int, 1>{});
-    case 3: return f(std::integral_constant<int, 3>{});
-    default: return f(std::integral_constant<int, 2>{});
-  }
-}
 
 struct Vecs {
   std::vector<void*> ptrs;

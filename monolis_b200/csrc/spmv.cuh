@@ -2,6 +2,9 @@
 // shared by the standalone kernels and the fused solver kernels.
 #pragma once
 
+#include <cstdio>
+#include <type_traits>
+
 #include "common.cuh"
 #include "dev.h"
 
@@ -269,6 +272,31 @@ __device__ __forceinline__ void load_alu_rows(const T* __restrict__ alu, int N, 
 template <int B, class T>
 __device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int row, T (&t)[B]) {
   diag_solve<B, T>([&](int j, int k) { return alu[(long long)(j * B + k) * N + row]; }, t);
+}
+
+// Compile-time block size and unroll depth from their runtime values.
+template <class F>
+inline int dispatch_ndof(int ndof, F&& f) {
+  switch (ndof) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 2: return f(std::integral_constant<int, 2>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 5: return f(std::integral_constant<int, 5>{});
+    case 6: return f(std::integral_constant<int, 6>{});
+    default:
+      fprintf(stderr, "** monolis_b200: NDOF=%d is not supported on the device (1..6)\n", ndof);
+      return kBadInput;
+  }
+}
+
+template <class F>
+inline int dispatch_u(int u, F&& f) {
+  switch (u) {
+    case 1: return f(std::integral_constant<int, 1>{});
+    case 3: return f(std::integral_constant<int, 3>{});
+    default: return f(std::integral_constant<int, 2>{});
+  }
 }
 
 }  // namespace mb

@@ -214,6 +214,28 @@ def diffusion_kappa(m, n: int = 128, seed: int = 5, kappa=None):
     return b, kappa, kref, elem
 
 
+def face_x0_fixed(n: int, ndof: int) -> np.ndarray:
+    """Per-dof mask (int32, n^3 * ndof) of the dofs clamped on the x = 0 face."""
+    fixed = np.zeros((n ** 3, ndof), dtype=np.int32)
+    fixed[0::n, :] = 1
+    return fixed.reshape(-1)
+
+
+def smooth_target(n: int, seed: int = 5) -> np.ndarray:
+    """x_target of the adjoint workload on the n^3 node grid of the unit cube:
+    sin(pi x) sin(pi y) sin(pi z) plus 0.1 times a seeded smooth field (eight
+    low-frequency sine modes with N(0,1) amplitudes)."""
+    t = np.linspace(0.0, 1.0, n)
+    z, y, x = np.meshgrid(t, t, t, indexing="ij")  # node id = ix + n*iy + n*n*iz
+    field = np.zeros_like(x)
+    amp = normal(seed + 1000, 8)
+    modes = [(1, 2, 1), (2, 1, 1), (1, 1, 2), (2, 2, 1), (1, 2, 2), (2, 1, 2), (3, 1, 1), (1, 3, 2)]
+    for a, (kx, ky, kz) in zip(amp, modes):
+        field += a * np.sin(kx * np.pi * x) * np.sin(ky * np.pi * y) * np.sin(kz * np.pi * z)
+    out = np.sin(np.pi * x) * np.sin(np.pi * y) * np.sin(np.pi * z) + 0.1 * field
+    return np.ascontiguousarray(out.reshape(-1))
+
+
 def spmv_bytes(nz: int, n: int, ndof: int, value_bytes: int) -> int:
     """Algorithmic bytes of one block SpMV: every value and column id read
     once, the row offsets once, x read once and y written once."""
