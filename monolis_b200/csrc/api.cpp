@@ -523,10 +523,6 @@ bool method_supported(const MONOLIS* m) {
             str_prec(pc));
     return false;
   }
-  if (m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] == 1 && mth != MONOLIS_ITER_CG) {
-    fprintf(stderr, "** monolis_b200: mixed precision is provided for CG\n");
-    return false;
-  }
   return true;
 }
 

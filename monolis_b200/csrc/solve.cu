@@ -325,10 +325,13 @@ __global__ void __launch_bounds__(kThreads)
 // BiCGSTAB kernels (src/iterative/BiCGSTAB.f90:87-170)
 // ---------------------------------------------------------------------------
 // P = R + beta*(P - omega*V) (or P = R on iteration 1); PT = M^-1 P.
+// Mixed precision (x64 != null): after a refresh it also folds the FP32
+// correction into the FP64 solution, X += Y, Y = 0, for its block's rows.
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_p_kernel(int N, T* __restrict__ p, const T* __restrict__ r, const T* __restrict__ vv,
-                  T* __restrict__ pt, const T* __restrict__ alu, int prec, const SolverState* st) {
+                  T* __restrict__ pt, const T* __restrict__ alu, int prec, const SolverState* st,
+                  double* __restrict__ x64 = nullptr, T* __restrict__ yacc = nullptr) {
   constexpr bool kStage = B <= 3;
   constexpr int kS = kStage ? kThreads * B : 1;
   __shared__ T sp[kS], sr[kS], sv[kS];
@@ -338,6 +341,14 @@ __global__ void __launch_bounds__(kThreads)
   const long long row0 = (long long)blockIdx.x * kThreads;
   const int nrows = (int)min((long long)kThreads, N - row0);
   const int row = (int)row0 + threadIdx.x;
+  if (x64 && st->fold && threadIdx.x < nrows) {
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = (long long)row * B + c;
+      x64[i] += (double)yacc[i];
+      yacc[i] = (T)0;
+    }
+  }
   if (kStage) {
     stage_in<T, B>(sr, r, row0, nrows);
     if (!first) {
@@ -465,7 +476,9 @@ __global__ void __launch_bounds__(kThreads)
 
 // X = X + alpha*PT + omega*ST; R = -omega*T + S; <R,R>, <R,RT>
 // (BiCGSTAB.f90:148-164). On iter % iter_RR == 0 only X is updated here.
-template <int B, class T>
+__device__ void fin_mixed_bicg(SolverState* st, double rr, double rrt, double* hist);
+
+template <int B, class T, bool Mixed = false>
 __global__ void __launch_bounds__(kThreads)
     bicg_xr_kernel(int N, T* __restrict__ x, const T* __restrict__ pt, const T* __restrict__ stv,
                    T* __restrict__ r, const T* __restrict__ s, const T* __restrict__ t, const T* __restrict__ rt,
@@ -488,7 +501,10 @@ __global__ void __launch_bounds__(kThreads)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
     return;
   }
-  grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_bicg(st, tot[0], tot[1], hist); });
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (Mixed) fin_mixed_bicg(st, tot[0], tot[1], hist);
+    else fin_bicg(st, tot[0], tot[1], hist);
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -519,6 +535,89 @@ __device__ void fin_mixed_inner(SolverState* st, double rr, double rz, double* h
   st->rho = rz;
   st->beta = st->rho / st->rho1;
   st->iter += 1;
+}
+
+// Mixed precision BiCGSTAB: the same scheme on src/iterative/BiCGSTAB.f90's
+// recurrences. X + Y is the solution (Y accumulates alpha*PT + omega*ST in
+// FP32); a refresh recomputes R = B - A (X + Y) in FP64 and continues with
+// rho = <R,RT> of that residual, the shadow residual RT and P, V unchanged
+// (the reference's own true-residual replacement, made adaptive).
+__device__ void fin_mixed_bicg(SolverState* st, double rr, double rrt, double* hist) {
+  const double rn = sqrt(rr);
+  const double resid = sqrt(rr / st->B2);
+  record(st, hist, resid);
+  st->rho1 = st->rho;
+  if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
+  if (rn > st->rmax) st->rmax = rn;
+  if (rn < st->delta * st->rmax || resid < st->tol || st->iter >= st->max_iter ||
+      (st->period > 0 && st->iter - st->last_refresh >= st->period)) {
+    st->refresh = 1;
+    return;
+  }
+  st->rho = rrt;
+  if (rrt == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+  st->beta = (st->rho / st->rho1) * (st->alpha / st->omega);
+  st->iter += 1;
+}
+
+// V = A PT (FP32 paired layout); c2 = <RT,V>; alpha = rho/c2.
+template <int B, int U>
+__global__ void __launch_bounds__(kThreads)
+    mbicg_v_kernel(SellView2 A, const float* __restrict__ pt, float* __restrict__ vv, const float* __restrict__ rt,
+                   double* partials, unsigned int* ticket, SolverState* st) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  const int npairs = (A.N + 1) / 2;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
+    float y0[B], y1[B];
+    sell_row2<B, U>(A, pt, t, y0, y1);
+    const int nr = (2 * t + 1 < A.N) ? 2 : 1;
+    for (int h = 0; h < nr; h++) {
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        const long long i = (long long)(2 * t + h) * B + c;
+        const float yv = h ? y1[c] : y0[c];
+        vv[i] = yv;
+        v[0] += (double)rt[i] * (double)yv;
+      }
+    }
+  }
+  grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    st->c2 = tot[0];
+    st->fold = 0;  // the p kernel of this iteration has folded y
+    if (tot[0] == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+    st->alpha = st->rho / tot[0];
+  });
+}
+
+// T = A ST (FP32 paired layout); (T,S), (T,T); omega.
+template <int B, int U>
+__global__ void __launch_bounds__(kThreads)
+    mbicg_t_kernel(SellView2 A, const float* __restrict__ stv, float* __restrict__ t, const float* __restrict__ s,
+                   double* partials, unsigned int* ticket, SolverState* st) {
+  if (st->done) return;
+  double v[2] = {0.0, 0.0};
+  const int npairs = (A.N + 1) / 2;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += gridDim.x * blockDim.x) {
+    float y0[B], y1[B];
+    sell_row2<B, U>(A, stv, q, y0, y1);
+    const int nr = (2 * q + 1 < A.N) ? 2 : 1;
+    for (int h = 0; h < nr; h++) {
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        const long long i = (long long)(2 * q + h) * B + c;
+        const float yv = h ? y1[c] : y0[c];
+        t[i] = yv;
+        v[0] += (double)yv * (double)s[i];
+        v[1] += (double)yv * (double)yv;
+      }
+    }
+  }
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    st->ts = tot[0];
+    st->tt = tot[1];
+    st->omega = tot[1] == 0.0 ? 0.0 : tot[0] / tot[1];
+  });
 }
 
 // P = Z + beta*P in FP32 (P = Z on iteration 1), and after a refresh the
@@ -681,13 +780,16 @@ __global__ void __launch_bounds__(kThreads)
 // initial residual (iter == 0) and when the update kernel raised `refresh`;
 // it sits in every iteration on a small grid, so the common case (nothing
 // to do) costs one flag read per block.
-template <int B>
+// BiCGSTAB mode (Bicg): the second dot is <r,rt> and the initial refresh
+// also sets the shadow residual rt = r (z unused).
+template <int B, bool Bicg = false>
 __global__ void __launch_bounds__(kThreads)
     mixed_refresh_kernel(SellView<double> A, const double* __restrict__ x, const float* __restrict__ y,
                          const double* __restrict__ b, float* __restrict__ r, float* __restrict__ z,
                          const float* __restrict__ alu, int prec, double* partials, unsigned int* ticket,
-                         SolverState* st, double* hist) {
+                         SolverState* st, double* hist, float* __restrict__ rt = nullptr) {
   if (st->done || !(st->iter == 0 || st->refresh)) return;
+  const bool init = st->iter == 0;
   constexpr int B2 = B * B;
   double v[2] = {0.0, 0.0};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
@@ -719,11 +821,21 @@ __global__ void __launch_bounds__(kThreads)
       r[i] = t[c];
       w[c] = t[c];
     }
-    if (prec) diag_row<B, float>(alu, A.N, row, w);
+    if (Bicg) {
 #pragma unroll
-    for (int c = 0; c < B; c++) {
-      z[(long long)row * B + c] = w[c];
-      v[1] += (double)t[c] * (double)w[c];
+      for (int c = 0; c < B; c++) {
+        const long long i = (long long)row * B + c;
+        float rtv;
+        if (init) { rt[i] = t[c]; rtv = t[c]; } else { rtv = rt[i]; }
+        v[1] += (double)t[c] * (double)rtv;
+      }
+    } else {
+      if (prec) diag_row<B, float>(alu, A.N, row, w);
+#pragma unroll
+      for (int c = 0; c < B; c++) {
+        z[(long long)row * B + c] = w[c];
+        v[1] += (double)t[c] * (double)w[c];
+      }
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
@@ -747,7 +859,12 @@ __global__ void __launch_bounds__(kThreads)
     if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
     st->rmax = sqrt(rr);
     st->rho = rz;
-    st->beta = st->rho / st->rho1;
+    if (Bicg) {
+      if (rz == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+      st->beta = (st->rho / st->rho1) * (st->alpha / st->omega);
+    } else {
+      st->beta = st->rho / st->rho1;
+    }
     st->iter += 1;
   });
 }
@@ -807,10 +924,6 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
   if (p.method != 1 && p.method != 5) return kBadInput;
-  if (p.precision == 1 && p.method != 1) {
-    fprintf(stderr, "** monolis_b200: mixed precision is implemented for CG\n");
-    return kBadInput;
-  }
   int rc = scratch_ensure(sc, (size_t)p.max_iter + 2);
   if (rc) return rc;
   if (p.precision == 1) {
@@ -833,7 +946,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   SolverState h{};
   h.tol = p.tol;
   h.max_iter = p.max_iter;
-  h.iter_rr = iter_rr;
+  h.iter_rr = p.precision == 1 ? 0x7fffffff : iter_rr;  // mixed: refreshes replace the fixed schedule
   h.period = p.precision == 1 ? p.refresh_period : 0;
   h.delta = p.delta > 0 ? p.delta : 0.1;
   MB_CUDA_OK(cudaMemcpyAsync(sc.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
@@ -911,6 +1024,41 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           if (ev) cudaEventRecord(ev[6], ss);
         };
       }
+    } else if (p.method == 5) {
+      SellView2 A32 = view2_of(m);
+      const float* alu32 = m.d_alu32;
+      float *r = vec.get<float>(n), *rt = vec.get<float>(n), *pp = vec.get<float>(n), *pt = vec.get<float>(n),
+            *sv = vec.get<float>(n), *stv = vec.get<float>(n), *t = vec.get<float>(n), *vv = vec.get<float>(n),
+            *y = vec.get<float>(n);
+      if (!r || !rt || !pp || !pt || !sv || !stv || !t || !vv || !y) return kCudaError;
+      double* x = d_x;
+      const double* b = d_b;
+      auto k_v = mbicg_v_kernel<B, U>;
+      auto k_t = mbicg_t_kernel<B, U>;
+      auto k_xr = bicg_xr_kernel<B, float, true>;
+      auto k_ref = mixed_refresh_kernel<B, true>;
+      const int g_v = row_grid((N + 1) / 2), g_t = g_v, g_xr = pgrid(k_xr), g_ref = row_grid(N);
+      if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
+      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
+      plan.kernels = 6;
+      plan.always_all = true;
+      plan.kind = {2, 0, 2, 0, 1, 0};
+      plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
+        if (ev) cudaEventRecord(ev[0], ss);
+        bicg_p_kernel<B, float><<<gb, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu32, prec, st, x, y);
+        if (ev) cudaEventRecord(ev[1], ss);
+        k_v<<<g_v, kThreads, 0, ss>>>(A32, pt, vv, rt, partials, ticket, st);
+        if (ev) cudaEventRecord(ev[2], ss);
+        bicg_s_kernel<B, float><<<gb, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu32, prec, st);
+        if (ev) cudaEventRecord(ev[3], ss);
+        k_t<<<g_t, kThreads, 0, ss>>>(A32, stv, t, sv, partials, ticket, st);
+        if (ev) cudaEventRecord(ev[4], ss);
+        k_xr<<<g_xr, kThreads, 0, ss>>>(N, y, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+        if (ev) cudaEventRecord(ev[5], ss);
+        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
+        if (ev) cudaEventRecord(ev[6], ss);
+      };
+      plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n, x, y, st); };
     } else {
       SellView2 A32 = view2_of(m);
       const float* alu32 = m.d_alu32;
@@ -925,7 +1073,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       const int g_spmv = row_grid((N + 1) / 2), g_upd = pgrid(k_upd);
       const int g_ref = row_grid(N);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
-      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
+      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
       plan.kernels = 4;
       plan.always_all = true;
       plan.kind = {1, 0, 2, 0};
@@ -937,7 +1085,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (ev) cudaEventRecord(ev[2], ss);
         k_upd<<<g_upd, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist);
         if (ev) cudaEventRecord(ev[3], ss);
-        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist);
+        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
         if (ev) cudaEventRecord(ev[4], ss);
       };
       plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n, x, y, st); };

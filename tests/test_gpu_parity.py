@@ -190,6 +190,33 @@ def test_cg_mixed_precision(gpu, oracle):
     assert rel_err(xm, xo) < 1e-5
 
 
+@pytest.mark.parametrize("n,peclet", [(8, 0.5), (12, 5.0), (16, 50.0), (24, 5.0), (32, 0.5)])
+@pytest.mark.parametrize("prec", [api.PREC_DIAG, api.PREC_NONE])
+def test_bicgstab_mixed_precision(gpu, oracle, n, peclet, prec):
+    """FP32-inner BiCGSTAB with FP64 refreshes on the nonsymmetric
+    convection-diffusion systems: converged on the true FP64 residual
+    (checked with the oracle's SpMV) and within 1e-5 of the FP64 solution."""
+    mp, b = build(gpu, "convection_diffusion", n=n, peclet=peclet)
+    mo, _ = build(oracle, "convection_diffusion", n=n, peclet=peclet)
+    xo, _, _, st_o = solve(mo, b, api.ITER_BICGSTAB, prec, tol=1e-12)
+    xm, it_m, res_m, st_m = solve(mp, b, api.ITER_BICGSTAB, prec, tol=1e-8, precision=1)
+    assert st_o == 0 and st_m == 0 and res_m < 1e-8
+    r = b - mo.matvec(xm)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1.01e-8
+    assert mp.Iarray[api.B200_PRM_I_N_REFINE] >= 1
+    assert rel_err(xm, xo) < 1e-5
+
+
+def test_bicgstab_mixed_tight_tolerance(gpu, oracle):
+    """Refinement carries the solution well past FP32 accuracy (1e-11)."""
+    mp, b = build(gpu, "convection_diffusion", n=20, peclet=5.0)
+    mo, _ = build(oracle, "convection_diffusion", n=20, peclet=5.0)
+    xo, _, _, _ = solve(mo, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=1e-13)
+    xm, _, res_m, st_m = solve(mp, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=1e-11, precision=1)
+    assert st_m == 0 and res_m < 1e-11
+    assert rel_err(xm, xo) < 1e-8
+
+
 def test_zero_rhs(gpu, oracle):
     # src/linalg/mat_converge.f90:40-48: <r0,r0> == 0 -> X = 0, converged
     for lib in (gpu, oracle):
