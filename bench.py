@@ -108,13 +108,193 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def oracle_iterations(n):
+def fixture():
     try:
         with open(FIXTURE) as f:
-            d = json.load(f)
-        return d.get(f"elasticity_n{n}_cg_diag_tol1e-08")
+            return json.load(f)
     except (OSError, ValueError):
-        return None
+        return {}
+
+
+def oracle_iterations(n):
+    return fixture().get(f"elasticity_n{n}_cg_diag_tol1e-08")
+
+
+def device_solve_timed(m, stream, d_b, d_x):
+    """One device-resident solve timed with CUDA events on the library stream."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    rc = m.device_solve(d_b.data_ptr(), d_x.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"solve failed: {api.STATUS_NAMES.get(rc, rc)}")
+    return e0.elapsed_time(e1) * 1e-3
+
+
+def kernel_times(m, stream, d_b, d_x):
+    """Per-kernel average seconds of one solve in the library's kernel-timer
+    mode (every kernel bracketed by CUDA events on the library stream)."""
+    m.Iarray[api.B200_PRM_I_KERNEL_TIMERS] = 1
+    try:
+        device_solve_timed(m, stream, d_b, d_x)
+    finally:
+        m.Iarray[api.B200_PRM_I_KERNEL_TIMERS] = 0
+    it = max(m.get_converge_iter(), 1)
+    return [m.Rarray[api.B200_PRM_R_TIME_KERNEL + k] / it for k in range(8)], it
+
+
+def workload_c3(lib, args, peak):
+    """Nonsymmetric 7-point upwind convection-diffusion, 256^3 unknowns,
+    BiCGSTAB + DIAG to 1e-8: FP64 and FP32-refined, three cell Peclet numbers."""
+    import torch
+    fx = fixture()
+    out = {}
+    for pe in args.c3_peclet:
+        m = api.Monolis(lib)
+        t0 = time.perf_counter()
+        b = problems.convection_diffusion(m, n=args.c3_n, peclet=pe)
+        t_asm = time.perf_counter() - t0
+        m.quiet()
+        m.set_error_abort(False)
+        m.set_method(api.ITER_BICGSTAB)
+        m.set_precond(api.PREC_DIAG)
+        m.set_tolerance(TOL)
+        m.set_maxiter(20000)
+        m.set_matrix_cache(True)
+        stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+        d_b = torch.from_numpy(b).cuda()
+        d_x = torch.zeros_like(d_b)
+        res = {}
+        for prec, name in ((0, "fp64"), (1, "mixed")):
+            m.set_precision(prec)
+            m.device_prepare()
+            device_solve_timed(m, stream, d_b, d_x)  # warm-up
+            t = device_solve_timed(m, stream, d_b, d_x)
+            d_r = torch.empty_like(d_x)
+            m.device_matvec(d_x.data_ptr(), d_r.data_ptr())
+            stream.synchronize()
+            res[name] = {"s": t, "iterations": m.get_converge_iter(),
+                         "true_rel_residual": (torch.linalg.norm(d_b - d_r) / torch.linalg.norm(d_b)).item(),
+                         "fp64_refreshes": int(m.Iarray[api.B200_PRM_I_N_REFINE])}
+            if prec == 0:
+                x64 = d_x.clone()
+                kt, _ = kernel_times(m, stream, d_b, d_x)
+                res[name]["kernel_us_per_iteration"] = {"p": kt[0] * 1e6, "v=A*pt": kt[1] * 1e6, "s": kt[2] * 1e6,
+                                                        "t=A*st": kt[3] * 1e6, "x,r": kt[4] * 1e6}
+                byts = problems.spmv_bytes(m.NZ, m.N, 1, 8)
+                res[name]["spmv_in_solve_gbs"] = byts / kt[1] / 1e9
+                res[name]["spmv_in_solve_frac_of_measured"] = byts / kt[1] / 1e9 / peak
+        res["mixed"]["rel_error_vs_fp64_solution"] = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
+        key = f"convection_diffusion_n{args.c3_n}_pe{pe:g}_bicgstab_diag_tol1e-08"
+        out[f"pe{pe:g}"] = {"assembly_s": t_asm, **res, "speedup_mixed_vs_fp64": res["fp64"]["s"] / res["mixed"]["s"],
+                            "oracle_iterations": fx.get(key), "oracle_iterations_by_threads": fx.get(key + ":by_threads")}
+        m.finalize()
+        del d_b, d_x, x64
+    return {"workload": f"3D upwind convection-diffusion {args.c3_n}^3 unknowns, ndof=1, BiCGSTAB + DIAG, "
+                        f"rel.res 1e-8, FP64 vs FP32-inner/FP64-refined", "by_peclet": out}
+
+
+def workload_c5(lib, args):
+    """Adjoint gradient of L = 1/2 ||x - x_target||^2 for 3D Q1 diffusion with
+    per-element log-normal conductivity (128^3 nodes): forward CG to 1e-10,
+    transpose solve, per-element gradient; FP64 and FP32-refined, plus
+    central differences on a few seeded directions."""
+    import torch
+    n = args.c5_n
+    m = api.Monolis(lib)
+    t0 = time.perf_counter()
+    b, kappa, kref, elem = problems.diffusion_kappa(m, n=n)
+    t_asm = time.perf_counter() - t0
+    target = problems.smooth_target(n)
+    fixed = problems.face_x0_fixed(n, 1)
+    m.quiet()
+    m.set_error_abort(False)
+    m.set_method(api.ITER_CG)
+    m.set_precond(api.PREC_DIAG)
+    m.set_tolerance(1e-10)
+    m.set_maxiter(20000)
+    m.set_matrix_cache(True)
+    stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+    d_b = torch.from_numpy(b).cuda()
+    d_t = torch.from_numpy(target).cuda()
+    d_elem = torch.from_numpy(np.ascontiguousarray(elem)).cuda()
+    d_k = torch.from_numpy(np.ascontiguousarray(kref.reshape(-1))).cuda()
+    d_fix = torch.from_numpy(fixed).cuda()
+    n_elem = len(elem)
+    res = {}
+    grads = {}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        m.set_precision(prec)
+        m.device_prepare()
+        d_x = torch.zeros_like(d_b)
+        d_lam = torch.zeros_like(d_b)
+        d_g = torch.empty(n_elem, dtype=torch.float64, device="cuda")
+        for rep in range(2):  # warm-up, then timed
+            t_fwd = device_solve_timed(m, stream, d_b, d_x)
+            it_f = m.get_converge_iter()
+            d_rhs = d_x - d_t
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc = lib.monolis_b200_device_solve_transpose_R(m.p, d_rhs.data_ptr(), d_lam.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            if rc:
+                raise RuntimeError(f"adjoint solve failed: {rc}")
+            t_adj = e0.elapsed_time(e1) * 1e-3
+            it_a = m.get_converge_iter()
+            e0.record(stream)
+            for _ in range(10):
+                rc = lib.monolis_b200_device_element_gradient_R(m.p, n_elem, 8, d_elem.data_ptr(), d_k.data_ptr(), 0,
+                                                               d_lam.data_ptr(), d_x.data_ptr(), d_fix.data_ptr(),
+                                                               -1.0, d_g.data_ptr())
+            e1.record(stream)
+            e1.synchronize()
+            if rc:
+                raise RuntimeError(f"element gradient failed: {rc}")
+            t_grad = e0.elapsed_time(e1) * 1e-3 / 10
+        grads[name] = d_g.cpu().numpy()
+        gbytes = n_elem * (8 * 4 + 8) + 3 * (n ** 3) * 8  # connectivity, gradient, lambda + x + mask once
+        res[name] = {"forward_s": t_fwd, "forward_iterations": it_f, "adjoint_s": t_adj, "adjoint_iterations": it_a,
+                     "gradient_kernel_us": t_grad * 1e6, "gradient_kernel_gbs": gbytes / t_grad / 1e9,
+                     "total_s": t_fwd + t_adj + t_grad}
+        if prec == 0:
+            x_ref = d_x.cpu().numpy()
+    g64 = grads["fp64"]
+    res["mixed"]["gradient_rel_diff_vs_fp64"] = float(np.linalg.norm(grads["mixed"] - g64) / np.linalg.norm(g64))
+    fd = []
+    if args.c5_fd_dirs > 0:
+        # central differences through the public API: assemble A(kappa +- h d) on the host, solve on the GPU
+        rng = np.random.default_rng(2025)
+        h = 1e-4
+
+        def loss(kap):
+            mm = api.Monolis(lib)
+            bb, _, _, _ = problems.diffusion_kappa(mm, n=n, kappa=kap)
+            mm.quiet()
+            mm.set_error_abort(False)
+            mm.set_method(api.ITER_CG)
+            mm.set_precond(api.PREC_DIAG)
+            mm.set_tolerance(1e-12)
+            mm.set_maxiter(50000)
+            xx = np.zeros_like(bb)
+            mm.solve(bb, xx)
+            mm.finalize()
+            return 0.5 * float(np.dot(xx - target, xx - target))
+        for _ in range(args.c5_fd_dirs):
+            d = kappa * rng.standard_normal(n_elem)
+            fdv = (loss(kappa + h * d) - loss(kappa - h * d)) / (2 * h)
+            an = float(np.dot(g64, d))
+            fd.append(abs(fdv - an) / abs(an))
+    m.finalize()
+    return {"workload": f"adjoint of L=1/2||x-x_target||^2, 3D Q1 diffusion {n}^3 nodes, log-normal kappa per element "
+                        f"({n_elem} elements), forward/adjoint CG+DIAG to 1e-10",
+            "assembly_s": t_asm, "loss": 0.5 * float(np.dot(x_ref - target, x_ref - target)), **res,
+            "fd_directions": len(fd), "fd_max_rel_err_fp64": max(fd) if fd else None}
 
 
 def run_reference(args, rank):
@@ -173,6 +353,13 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workloads", default="c3,c5", help="secondary workloads to run after the headline (c3,c5 or none)")
+    ap.add_argument("--c3-n", type=int, default=256)
+    ap.add_argument("--c3-peclet", type=float, nargs="+", default=[0.5, 5.0, 50.0])
+    ap.add_argument("--c5-n", type=int, default=128)
+    ap.add_argument("--c5-fd-dirs", type=int, default=2)
+    ap.add_argument("--traffic-per-launch", type=float, default=None,
+                    help="DRAM bytes per launch of the dominant kernel from an ncu capture (reported as-is)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,6 +439,14 @@ def main():
     torch.cuda.nvtx.range_pop()
     barrier()
     clocks = clk.summary()
+    # per-kernel durations inside a solve (kernel-timer mode, one extra solve
+    # of each precision, after the timed steps)
+    x_mixed = d_x.clone()
+    kt32, _ = kernel_times(m, stream, d_b, d_x)
+    m.set_precision(0)
+    kt64, _ = kernel_times(m, stream, d_b, d_x)
+    m.set_precision(1)
+    d_x.copy_(x_mixed)
     t_mixed = float(np.mean(times))
     nref = int(m.Iarray[api.B200_PRM_I_N_REFINE])
     err_vs_fp64 = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
@@ -343,8 +538,29 @@ def main():
         except Exception as e:  # report, do not hide
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
+    workloads = {}
+    if rank == 0 and world == 1:
+        for w in [w for w in args.workloads.split(",") if w and w != "none"]:
+            try:
+                if w == "c3":
+                    workloads["c3"] = workload_c3(lib, args, peak)
+                elif w == "c5":
+                    workloads["c5"] = workload_c5(lib, args)
+            except Exception as e:  # report, do not hide
+                workloads[w] = {"failed": repr(e)}
+            log(f"[rank 0] workload {w}: {json.dumps(workloads[w])[:400]}")
+
     if rank == 0:
-        dom = spmv["fp32"]
+        spmv32_bytes = problems.spmv_bytes(nz, N, nd, 4)
+        spmv64_bytes = problems.spmv_bytes(nz, N, nd, 8)
+        in_solve = {
+            "mixed_us_per_iteration": {"p+fold": kt32[0] * 1e6, "q=A*p (fp32, +<p,q>)": kt32[1] * 1e6,
+                                       "update (+M^-1, dots)": kt32[2] * 1e6, "refresh (gated)": kt32[3] * 1e6},
+            "fp64_us_per_iteration": {"p": kt64[0] * 1e6, "q=A*p (+<p,q>)": kt64[1] * 1e6,
+                                      "update (+M^-1, dots)": kt64[2] * 1e6, "residual (gated)": kt64[3] * 1e6},
+            "spmv_fp32_in_solve_gbs": spmv32_bytes / kt32[1] / 1e9,
+            "spmv_fp64_in_solve_gbs": spmv64_bytes / kt64[1] / 1e9,
+        }
         line = {
             "metric": METRIC, "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3, "higher_is_better": False,
@@ -361,10 +577,13 @@ def main():
             "spmv": {k: {"gbs": v["gbs"], "us": v["seconds"] * 1e6, "bytes": v["bytes"],
                          "frac_of_measured": v["gbs"] / peak, "frac_of_8tbs": v["gbs"] / 8000.0}
                      for k, v in spmv.items()},
-            "roofline": {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": dom["gbs"] / peak, "traffic": None,
-                         "kernel": "FP32 sliced-ELL block SpMV (ndof 3), standalone launch",
-                         "peak_kind": peak_kind},
+            "roofline": {"bound": "hbm", "achieved": in_solve["spmv_fp32_in_solve_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": in_solve["spmv_fp32_in_solve_gbs"] / peak,
+                         "traffic": args.traffic_per_launch,
+                         "kernel": "cg_spmv2_kernel (FP32 paired sliced-ELL SpMV q=A*p with fused <p,q>), "
+                                   "average launch inside a mixed solve, kernel-timer mode",
+                         "algorithmic_bytes_per_launch": spmv32_bytes, "peak_kind": peak_kind},
+            "in_solve_kernels": in_solve,
             "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call"},
             "gpu_launches": launches,
@@ -372,6 +591,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "assembly_s": t_asm,
+            "workloads": workloads,
         }
         print(json.dumps(line), flush=True)
     m.finalize()

@@ -43,7 +43,7 @@ static const int MONOLIS_B200_PRM_I_REFRESH_PERIOD = 41; /* mixed precision: FP6
 
 static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
                                                             below delta * its largest value since the last one
-                                                            (0: 0.1) */
+                                                            (0: 0.1 for CG, 0.01 for BiCGSTAB) */
 static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */
 static const int MONOLIS_B200_PRM_R_TIME_D2H       = 32; /* out: seconds spent on device->host copies */
 static const int MONOLIS_B200_PRM_R_TIME_LOOP      = 33; /* out: seconds in the device iteration loop */

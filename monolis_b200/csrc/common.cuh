@@ -38,11 +38,22 @@ __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p);
 __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 __device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }
 
-// ---- deterministic one-pass grid reduction of K doubles.
-// Every block writes its K partial sums to partials[block*K + k]; the last
-// block to arrive (atomic ticket) sums all partials in a fixed order and
-// runs `fin` on thread 0. The ticket is reset by the last block, so the same
-// scratch is reusable by the next stream-ordered launch.
+// ---- deterministic one-pass grid reduction of K doubles, two levels.
+// Every block writes its K partial sums to partials[block*K + k]. Blocks are
+// grouped by kReduceGroup consecutive indices; the last block of a group to
+// arrive (atomic ticket[1 + group]) sums that group's partials in index order
+// into partials[(gridDim.x + group)*K + k], and the last group to finish
+// (atomic ticket[0]) sums the group sums in index order and runs `fin` on
+// thread 0. Each finishing block reads at most kReduceGroup values, one per
+// thread, so the tail of the reduction stays short at any grid size, and the
+// result does not depend on the order in which blocks arrive. The tickets
+// are reset by the blocks that consumed them, so the same scratch serves the
+// next stream-ordered launch.
+//   partials: >= (gridDim.x + ceil(gridDim.x / kReduceGroup)) * K doubles
+//   ticket:   >= 1 + ceil(gridDim.x / kReduceGroup) zero-initialised words
+constexpr int kReduceGroup = 256;
+constexpr int kTicketWords = 1 + 65536 / kReduceGroup;  // grids up to 65536 blocks
+
 template <int K>
 __device__ __forceinline__ void block_sum(double (&v)[K], double* smem /* >= 32*K */) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -72,12 +83,17 @@ __device__ __forceinline__ void grid_reduce(double (&v)[K], double* partials, un
   __shared__ double smem[32 * K];
   __shared__ bool am_last;
   block_sum<K>(v, smem);
+  const unsigned int G = gridDim.x;
+  const unsigned int ngroups = (G + kReduceGroup - 1) / kReduceGroup;
+  const unsigned int g = blockIdx.x / kReduceGroup;
+  const unsigned int g0 = g * kReduceGroup;
+  const unsigned int gsize = min((unsigned int)kReduceGroup, G - g0);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < K; k++) partials[(size_t)blockIdx.x * K + k] = v[k];
     __threadfence();
-    unsigned int t = atomicAdd(ticket, 1u);
-    am_last = (t == gridDim.x - 1);
+    const unsigned int t = atomicAdd(ticket + 1 + g, 1u);
+    am_last = (t == gsize - 1);
   }
   __syncthreads();
   if (!am_last) return;
@@ -85,9 +101,28 @@ __device__ __forceinline__ void grid_reduce(double (&v)[K], double* partials, un
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k] = 0.0;
-  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+  for (unsigned int b = threadIdx.x; b < gsize; b += blockDim.x) {
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] += __ldcg(partials + (size_t)b * K + k);
+    for (int k = 0; k < K; k++) acc[k] += __ldcg(partials + (size_t)(g0 + b) * K + k);
+  }
+  block_sum<K>(acc, smem);
+  double* top = partials + (size_t)G * K;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) top[(size_t)g * K + k] = acc[k];
+    ticket[1 + g] = 0u;
+    __threadfence();
+    const unsigned int t = atomicAdd(ticket, 1u);
+    am_last = (t == ngroups - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k] = 0.0;
+  for (unsigned int b = threadIdx.x; b < ngroups; b += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < K; k++) acc[k] += __ldcg(top + (size_t)b * K + k);
   }
   block_sum<K>(acc, smem);
   if (threadIdx.x == 0) {

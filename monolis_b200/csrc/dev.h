@@ -125,7 +125,7 @@ struct SolveParams {
   double tol;
   int init_x;        // zero x before solving
   int precision;     // 0 FP64, 1 FP32 inner + FP64 reliable refresh
-  double delta;        // precision 1: refresh when ||r|| < delta * max ||r|| since the last one (0: 0.1)
+  double delta;        // precision 1: refresh when ||r|| < delta * max ||r|| since the last one (0: 0.1 CG, 0.01 BiCGSTAB)
   int refresh_period;  // precision 1: refresh at the latest every n iterations (0: no limit)
   int iter_rr;       // true residual every iter_rr iterations (reference: 200)
   int batch;         // iterations per graph launch

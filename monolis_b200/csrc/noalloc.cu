@@ -22,7 +22,7 @@
 namespace mb {
 namespace {
 
-// Capacity: one partial sum per block, blocks of 256 threads each reducing
+// Capacity: one partial sum per block (plus one per group of blocks), blocks of 256 threads each reducing
 // 4 elements per thread -> at most kNoAllocBlocks * 1024 elements.
 constexpr int kNoAllocThreads = 256;
 constexpr int kNoAllocPerThread = 4;
@@ -30,8 +30,8 @@ constexpr int kNoAllocBlocks = 16384;
 constexpr long long kNoAllocMaxN = (long long)kNoAllocBlocks * kNoAllocThreads * kNoAllocPerThread;
 
 struct NoAllocScratch {
-  double partials[kNoAllocBlocks];
-  unsigned int ticket;
+  double partials[kNoAllocBlocks + kNoAllocBlocks / kReduceGroup];  // block and group partial sums
+  unsigned int ticket[1 + kNoAllocBlocks / kReduceGroup];           // arrival tickets
 };
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
@@ -45,7 +45,7 @@ __global__ void dot_noalloc_kernel(long long n, const double* __restrict__ x, co
   double v[1] = {0.0};
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     v[0] += x[i] * y[i];
-  grid_reduce<1>(v, sc->partials, &sc->ticket, [&](double* tot) { *out = tot[0]; });
+  grid_reduce<1>(v, sc->partials, sc->ticket, [&](double* tot) { *out = tot[0]; });
 }
 
 }  // namespace
@@ -78,9 +78,9 @@ extern "C" int monolis_b200_inner_product_noalloc_R(long long n, const double* d
     sc = g_addr[dev];
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // the arrival ticket must start at zero (a previous call leaves it at
-  // zero; clearing it again costs nothing and recovers from an aborted call)
-  MB_CUDA_OK(cudaMemsetAsync(&sc->ticket, 0, sizeof(unsigned int), s));
+  // the arrival tickets must start at zero (a previous call leaves them at
+  // zero; clearing them again costs nothing and recovers from an aborted call)
+  MB_CUDA_OK(cudaMemsetAsync(sc->ticket, 0, sizeof(sc->ticket), s));
   long long blocks = (n + (long long)kNoAllocThreads * kNoAllocPerThread - 1) / ((long long)kNoAllocThreads * kNoAllocPerThread);
   if (blocks < 1) blocks = 1;
   dot_noalloc_kernel<<<(int)blocks, kNoAllocThreads, 0, s>>>(n, d_x, d_y, sc, d_sum);

@@ -426,8 +426,8 @@ int scratch_ensure(Scratch& sc, size_t hist_len) {
     sc.partials_cap = need;
   }
   if (!sc.ticket) {
-    MB_CUDA_OK(cudaMalloc((void**)&sc.ticket, 64 * sizeof(unsigned int)));
-    MB_CUDA_OK(cudaMemset(sc.ticket, 0, 64 * sizeof(unsigned int)));
+    MB_CUDA_OK(cudaMalloc((void**)&sc.ticket, kTicketWords * sizeof(unsigned int)));
+    MB_CUDA_OK(cudaMemset(sc.ticket, 0, kTicketWords * sizeof(unsigned int)));
   }
   if (!sc.st) MB_CUDA_OK(cudaMalloc((void**)&sc.st, sizeof(SolverState)));
   if (!sc.h_st) MB_CUDA_OK(cudaMallocHost((void**)&sc.h_st, 4 * sizeof(SolverState)));

@@ -3,10 +3,12 @@
 //
 // Every scalar of the recurrences (rho, alpha, beta, omega, B2, the
 // residual) lives in SolverState on the device. Each reduction is a one-pass
-// grid reduction whose last block also evaluates the scalar update, so an
-// iteration is a fixed sequence of kernels with no host round trip. Kernels
-// that reduce run on a persistent grid (as many blocks as fit on the GPU at
-// once), so the arrival ticket sees one atomic per resident block.
+// grid reduction (common.cuh) whose last block also evaluates the scalar
+// update, so an iteration is a fixed sequence of kernels with no host round
+// trip. Kernels that reduce run on a persistent grid (as many blocks as fit
+// on the GPU at once) and grid-stride over rows: at ndof 1 (7 blocks a row)
+// a block per 256 rows spends more time entering, reducing and leaving than
+// on its rows.
 //
 // The host captures `batch` iterations into a CUDA graph and launches it
 // repeatedly, reading the state word once per launch with two launches in
@@ -67,13 +69,6 @@ int pgrid(K kernel) {
   cache[key] = g;
   return g;
 }
-
-// Grid of a matrix kernel: one thread per row (or row pair), up to the
-// capacity of the reduction scratch, beyond which the kernels grid-stride.
-// The hardware block scheduler balances the uneven slice widths better than
-// a fixed grid-stride assignment does.
-constexpr int kMaxGrid = 65536;
-inline int row_grid(long long rows) { return (int)std::min<long long>(blocks_for(rows), kMaxGrid); }
 
 // ---------------------------------------------------------------------------
 // Scalar updates run by the last block of a grid reduction.
@@ -324,62 +319,85 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // BiCGSTAB kernels (src/iterative/BiCGSTAB.f90:87-170)
 // ---------------------------------------------------------------------------
+// Per-row DIAG apply of E = R*B values held in registers (R rows of B).
+template <int B, class T, int R>
+__device__ __forceinline__ void diag_rows(const T* __restrict__ alu, int N, long long row0, bool alu_vec,
+                                          T (&w)[R * B]) {
+  T L[B * B][R];
+  load_alu_rows<T, B, R>(alu, N, row0, alu_vec, L);
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    T t[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) t[c] = w[k * B + c];
+    diag_solve<B, T>([&](int j, int kk) { return L[j * B + kk][k]; }, t);
+#pragma unroll
+    for (int c = 0; c < B; c++) w[k * B + c] = t[c];
+  }
+}
+
 // P = R + beta*(P - omega*V) (or P = R on iteration 1); PT = M^-1 P.
 // Mixed precision (x64 != null): after a refresh it also folds the FP32
-// correction into the FP64 solution, X += Y, Y = 0, for its block's rows.
+// correction into the FP64 solution, X += Y, Y = 0. Register-blocked like
+// cg_update_kernel (the work vectors are the solver's own, 16-byte aligned).
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_p_kernel(int N, T* __restrict__ p, const T* __restrict__ r, const T* __restrict__ vv,
                   T* __restrict__ pt, const T* __restrict__ alu, int prec, const SolverState* st,
                   double* __restrict__ x64 = nullptr, T* __restrict__ yacc = nullptr) {
-  constexpr bool kStage = B <= 3;
-  constexpr int kS = kStage ? kThreads * B : 1;
-  __shared__ T sp[kS], sr[kS], sv[kS];
+  using RG = RowGroup<T, B>;
+  constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
   const bool first = st->iter == 1;
+  const bool fold = x64 && st->fold;
   const T beta = (T)st->beta, omega = (T)st->omega;
-  const long long row0 = (long long)blockIdx.x * kThreads;
-  const int nrows = (int)min((long long)kThreads, N - row0);
-  const int row = (int)row0 + threadIdx.x;
-  if (x64 && st->fold && threadIdx.x < nrows) {
-#pragma unroll
-    for (int c = 0; c < B; c++) {
-      const long long i = (long long)row * B + c;
-      x64[i] += (double)yacc[i];
-      yacc[i] = (T)0;
-    }
-  }
-  if (kStage) {
-    stage_in<T, B>(sr, r, row0, nrows);
+  const bool alu_vec = (N % R) == 0;
+  const long long ngroups = N / R;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  auto pval = [&](T rv, T pv, T vv_) { return first ? rv : add_rn(rv, mul_rn(beta, sub_rn(pv, mul_rn(omega, vv_)))); };
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
+    const long long row0 = g * R, e0 = row0 * B;
+    T rv[E], pv[E], w[E];
+    vload<T, E>(r + e0, rv);
     if (!first) {
-      stage_in<T, B>(sp, p, row0, nrows);
-      stage_in<T, B>(sv, vv, row0, nrows);
+      T vvv[E];
+      vload<T, E>(p + e0, pv);
+      vload<T, E>(vv + e0, vvv);
+#pragma unroll
+      for (int i = 0; i < E; i++) pv[i] = pval(rv[i], pv[i], vvv[i]);
+    } else {
+#pragma unroll
+      for (int i = 0; i < E; i++) pv[i] = rv[i];
     }
-    __syncthreads();
+    vstore<T, E>(p + e0, pv);
+#pragma unroll
+    for (int i = 0; i < E; i++) w[i] = pv[i];
+    if (prec) diag_rows<B, T, R>(alu, N, row0, alu_vec, w);
+    vstore<T, E>(pt + e0, w);
+    if (fold) {
+#pragma unroll
+      for (int i = 0; i < E; i++) {
+        x64[e0 + i] += (double)yacc[e0 + i];
+        yacc[e0 + i] = (T)0;
+      }
+    }
   }
-  if (threadIdx.x < nrows) {
+  for (long long row = ngroups * R + blockIdx.x * (long long)blockDim.x + threadIdx.x; row < N; row += stride) {
     T w[B];
 #pragma unroll
     for (int c = 0; c < B; c++) {
-      const int ls = threadIdx.x * B + c;
-      const long long i = (long long)row * B + c;
-      const T rv = kStage ? sr[ls] : r[i];
-      const T pv = first ? rv
-                         : add_rn(rv, mul_rn(beta, sub_rn(kStage ? sp[ls] : p[i], mul_rn(omega, kStage ? sv[ls] : vv[i]))));
-      if (kStage) sp[ls] = pv; else p[i] = pv;
+      const long long i = row * B + c;
+      const T pv = first ? r[i] : pval(r[i], p[i], vv[i]);
+      p[i] = pv;
       w[c] = pv;
+      if (fold) {
+        x64[i] += (double)yacc[i];
+        yacc[i] = (T)0;
+      }
     }
-    if (prec) diag_row<B, T>(alu, N, row, w);
+    if (prec) diag_row<B, T>(alu, N, (int)row, w);
 #pragma unroll
-    for (int c = 0; c < B; c++) {
-      if (kStage) sv[threadIdx.x * B + c] = w[c];
-      else pt[(long long)row * B + c] = w[c];
-    }
-  }
-  if (kStage) {
-    __syncthreads();
-    stage_out<T, B>(p, sp, row0, nrows);
-    stage_out<T, B>(pt, sv, row0, nrows);
+    for (int c = 0; c < B; c++) pt[row * B + c] = w[c];
   }
 }
 
@@ -407,45 +425,42 @@ __global__ void __launch_bounds__(kThreads)
   });
 }
 
-// S = -alpha*V + R; ST = M^-1 S (BiCGSTAB.f90:124-126)
+// S = -alpha*V + R; ST = M^-1 S (BiCGSTAB.f90:124-126). Register-blocked.
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_s_kernel(int N, T* __restrict__ s, const T* __restrict__ r, const T* __restrict__ vv,
                   T* __restrict__ stv, const T* __restrict__ alu, int prec, const SolverState* st) {
-  constexpr bool kStage = B <= 3;
-  constexpr int kS = kStage ? kThreads * B : 1;
-  __shared__ T sr[kS], sv[kS];
+  using RG = RowGroup<T, B>;
+  constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
   const T alpha = (T)st->alpha;
-  const long long row0 = (long long)blockIdx.x * kThreads;
-  const int nrows = (int)min((long long)kThreads, N - row0);
-  const int row = (int)row0 + threadIdx.x;
-  if (kStage) {
-    stage_in<T, B>(sr, r, row0, nrows);
-    stage_in<T, B>(sv, vv, row0, nrows);
-    __syncthreads();
+  const bool alu_vec = (N % R) == 0;
+  const long long ngroups = N / R;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
+    const long long row0 = g * R, e0 = row0 * B;
+    T rv[E], vvv[E], w[E];
+    vload<T, E>(r + e0, rv);
+    vload<T, E>(vv + e0, vvv);
+#pragma unroll
+    for (int i = 0; i < E; i++) rv[i] = axpy_rn(-alpha, vvv[i], rv[i]);
+    vstore<T, E>(s + e0, rv);
+#pragma unroll
+    for (int i = 0; i < E; i++) w[i] = rv[i];
+    if (prec) diag_rows<B, T, R>(alu, N, row0, alu_vec, w);
+    vstore<T, E>(stv + e0, w);
   }
-  if (threadIdx.x < nrows) {
+  for (long long row = ngroups * R + blockIdx.x * (long long)blockDim.x + threadIdx.x; row < N; row += stride) {
     T w[B];
 #pragma unroll
     for (int c = 0; c < B; c++) {
-      const int ls = threadIdx.x * B + c;
-      const long long i = (long long)row * B + c;
-      const T sval = axpy_rn(-alpha, kStage ? sv[ls] : vv[i], kStage ? sr[ls] : r[i]);
-      if (kStage) sr[ls] = sval; else s[i] = sval;
-      w[c] = sval;
+      const long long i = row * B + c;
+      w[c] = axpy_rn(-alpha, vv[i], r[i]);
+      s[i] = w[c];
     }
-    if (prec) diag_row<B, T>(alu, N, row, w);
+    if (prec) diag_row<B, T>(alu, N, (int)row, w);
 #pragma unroll
-    for (int c = 0; c < B; c++) {
-      if (kStage) sv[threadIdx.x * B + c] = w[c];
-      else stv[(long long)row * B + c] = w[c];
-    }
-  }
-  if (kStage) {
-    __syncthreads();
-    stage_out<T, B>(s, sr, row0, nrows);
-    stage_out<T, B>(stv, sv, row0, nrows);
+    for (int c = 0; c < B; c++) stv[row * B + c] = w[c];
   }
 }
 
@@ -483,12 +498,39 @@ __global__ void __launch_bounds__(kThreads)
     bicg_xr_kernel(int N, T* __restrict__ x, const T* __restrict__ pt, const T* __restrict__ stv,
                    T* __restrict__ r, const T* __restrict__ s, const T* __restrict__ t, const T* __restrict__ rt,
                    double* partials, unsigned int* ticket, SolverState* st, double* hist) {
+  constexpr int W = Vec16T<T>::n;  // elements per 16-byte access
   if (st->done) return;
   const bool rr_iter = (st->iter % st->iter_rr) == 0;
   const T alpha = (T)st->alpha, omega = (T)st->omega;
   const long long n = (long long)N * B;
+  // x is the caller's vector: 16-byte accesses only when it is aligned
+  const long long nv = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) ? n / W : 0;
+  const long long stride = (long long)gridDim.x * blockDim.x;
   double v[2] = {0.0, 0.0};
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv; q += stride) {
+    const long long i0 = q * W;
+    T xv[W], ptv[W], sv_[W];
+    vload<T, W>(x + i0, xv);
+    vload<T, W>(pt + i0, ptv);
+    vload<T, W>(stv + i0, sv_);
+#pragma unroll
+    for (int k = 0; k < W; k++) xv[k] = add_rn(add_rn(xv[k], mul_rn(alpha, ptv[k])), mul_rn(omega, sv_[k]));
+    vstore<T, W>(x + i0, xv);
+    if (!rr_iter) {
+      T tv[W], ssv[W], rtv[W];
+      vload<T, W>(t + i0, tv);
+      vload<T, W>(s + i0, ssv);
+      vload<T, W>(rt + i0, rtv);
+#pragma unroll
+      for (int k = 0; k < W; k++) {
+        tv[k] = axpy_rn(-omega, tv[k], ssv[k]);
+        v[0] += (double)tv[k] * (double)tv[k];
+        v[1] += (double)tv[k] * (double)rtv[k];
+      }
+      vstore<T, W>(r + i0, tv);
+    }
+  }
+  for (long long i = nv * W + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
     x[i] = add_rn(add_rn(x[i], mul_rn(alpha, pt[i])), mul_rn(omega, stv[i]));
     if (!rr_iter) {
       const T rv = axpy_rn(-omega, t[i], s[i]);
@@ -948,9 +990,11 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   h.max_iter = p.max_iter;
   h.iter_rr = p.precision == 1 ? 0x7fffffff : iter_rr;  // mixed: refreshes replace the fixed schedule
   h.period = p.precision == 1 ? p.refresh_period : 0;
-  h.delta = p.delta > 0 ? p.delta : 0.1;
+  // BiCGSTAB residual norms oscillate: a 0.1 drop below the running maximum
+  // comes every few iterations and would refresh needlessly
+  h.delta = p.delta > 0 ? p.delta : (p.method == 5 ? 0.01 : 0.1);
   MB_CUDA_OK(cudaMemcpyAsync(sc.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
-  MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * 64, s));
+  MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * kTicketWords, s));
   if (p.init_x) MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n, s));
 
   Vecs vec{{}, s};
@@ -973,13 +1017,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       double* x = d_x;
       const double* b = d_b;
       auto k_resid = resid_kernel<B, U, double, double>;
-      const int g_resid = row_grid(N);
+      const int g_resid = pgrid(k_resid);
       if (p.method == 1) {
         double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n), *pp = vec.get<double>(n);
         if (!r || !z || !q || !pp) return kCudaError;
         auto k_spmv = cg_spmv_kernel<B, U, double, double>;
         auto k_upd = cg_update_kernel<B, double>;
-        const int g_spmv = row_grid(N), g_upd = pgrid(k_upd);
+        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
         plan.kernels = 4;
         plan.kind = {1, 0, 2, 0};
@@ -1003,17 +1047,18 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_v = bicg_v_kernel<B, U, double, double>;
         auto k_t = bicg_t_kernel<B, U, double, double>;
         auto k_xr = bicg_xr_kernel<B, double>;
-        const int g_v = row_grid(N), g_t = row_grid(N), g_xr = pgrid(k_xr);
+        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
+        const int g_p = pgrid(bicg_p_kernel<B, double>), g_s = pgrid(bicg_s_kernel<B, double>);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
         plan.kernels = 6;
         plan.kind = {2, 0, 2, 0, 1, 0};
         plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
           if (ev) cudaEventRecord(ev[0], ss);
-          bicg_p_kernel<B, double><<<gb, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
+          bicg_p_kernel<B, double><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
           if (ev) cudaEventRecord(ev[1], ss);
           k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
           if (ev) cudaEventRecord(ev[2], ss);
-          bicg_s_kernel<B, double><<<gb, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
+          bicg_s_kernel<B, double><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
           if (ev) cudaEventRecord(ev[3], ss);
           k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
           if (ev) cudaEventRecord(ev[4], ss);
@@ -1037,7 +1082,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_t = mbicg_t_kernel<B, U>;
       auto k_xr = bicg_xr_kernel<B, float, true>;
       auto k_ref = mixed_refresh_kernel<B, true>;
-      const int g_v = row_grid((N + 1) / 2), g_t = g_v, g_xr = pgrid(k_xr), g_ref = row_grid(N);
+      const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr), g_ref = pgrid(k_ref);
+      const int g_p = pgrid(bicg_p_kernel<B, float>), g_s = pgrid(bicg_s_kernel<B, float>);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
       k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
       plan.kernels = 6;
@@ -1045,11 +1091,11 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       plan.kind = {2, 0, 2, 0, 1, 0};
       plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
         if (ev) cudaEventRecord(ev[0], ss);
-        bicg_p_kernel<B, float><<<gb, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu32, prec, st, x, y);
+        bicg_p_kernel<B, float><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu32, prec, st, x, y);
         if (ev) cudaEventRecord(ev[1], ss);
         k_v<<<g_v, kThreads, 0, ss>>>(A32, pt, vv, rt, partials, ticket, st);
         if (ev) cudaEventRecord(ev[2], ss);
-        bicg_s_kernel<B, float><<<gb, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu32, prec, st);
+        bicg_s_kernel<B, float><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu32, prec, st);
         if (ev) cudaEventRecord(ev[3], ss);
         k_t<<<g_t, kThreads, 0, ss>>>(A32, stv, t, sv, partials, ticket, st);
         if (ev) cudaEventRecord(ev[4], ss);
@@ -1070,8 +1116,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_spmv = cg_spmv2_kernel<B, U>;
       auto k_upd = mixed_update_kernel<B>;
       auto k_ref = mixed_refresh_kernel<B>;
-      const int g_spmv = row_grid((N + 1) / 2), g_upd = pgrid(k_upd);
-      const int g_ref = row_grid(N);
+      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+      const int g_ref = pgrid(k_ref);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
       k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
       plan.kernels = 4;
