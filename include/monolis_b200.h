@@ -150,6 +150,47 @@ int monolis_b200_device_element_gradient_R(MONOLIS* mat, int n_elem, int n_base,
                                            const double* d_x, const int* d_fixed_dof, double scale,
                                            double* d_grad);
 
+/* ---- batched solver: many independent systems in one persistent kernel ----
+ * No counterpart in the reference library (one system per monolis_solve_R).
+ * Systems are added from assembled MONOLIS structs (or raw block CSR: 0-based
+ * offsets and columns) and stacked on the device; each is solved by CG (+
+ * DIAG) with its own convergence test, all of them in one persistent kernel
+ * launched in thread-block clusters (one graph launch per solve). FP32 values
+ * and vectors inside the loop, FP64 dot products and scalars; refine = 1 adds
+ * FP64 reliable updates so that tol applies to the FP64 residual
+ * ||b - A x|| / ||b|| (refine = 0: FP32 recursion, tol 1e-6 class). Cluster
+ * size, CTA size and the system size below which systems are solved one per
+ * CTA are picked by timing candidates on the batch (autotune = 1) or set. */
+typedef struct monolis_b200_batch monolis_b200_batch;
+int  monolis_b200_batch_create(monolis_b200_batch** batch);
+void monolis_b200_batch_destroy(monolis_b200_batch* batch);
+/* copies the matrix; systems are numbered in the order they are added; all
+ * must have the same ndof */
+int  monolis_b200_batch_add_system(monolis_b200_batch* batch, MONOLIS* mat);
+int  monolis_b200_batch_add_csr(monolis_b200_batch* batch, int n, int ndof, const int* index, const int* item,
+                                const double* val);
+/* device layout, DIAG factors (precond MONOLIS_PREC_DIAG or NONE), tuning */
+int  monolis_b200_batch_prepare(monolis_b200_batch* batch, int precond, int autotune);
+int  monolis_b200_batch_set_config(monolis_b200_batch* batch, int cluster, int threads, long long split_rows);
+int  monolis_b200_batch_get_config(monolis_b200_batch* batch, int* cluster, int* threads, long long* split_rows);
+/* re-times the candidates with `iters` iterations each and keeps the fastest;
+ * on entry *n_candidates is the capacity of the output arrays, on return the
+ * number of candidates timed */
+int  monolis_b200_batch_autotune(monolis_b200_batch* batch, int iters, int* n_candidates, int* clusters,
+                                 int* threads, long long* split_rows, double* seconds);
+/* host b[i] / x[i] per system (x out); iter, resid (relative, FP64 true
+ * residual), status per system (MONOLIS_B200_* codes) */
+int  monolis_b200_batch_solve_R(monolis_b200_batch* batch, double** b, double** x, double tol, int max_iter,
+                                int refine, int* iter, double* resid, int* status);
+/* device-resident form: the stacked b and x (system i starts at offsets[i],
+ * in dofs; rows between systems are padding and stay zero) */
+int  monolis_b200_batch_info(monolis_b200_batch* batch, int* n_systems, long long* offsets);
+int  monolis_b200_batch_device_vectors(monolis_b200_batch* batch, double** d_b, double** d_x);
+int  monolis_b200_batch_device_solve_R(monolis_b200_batch* batch, double tol, int max_iter, int refine, int* iter,
+                                       double* resid, int* status);
+/* device seconds of the last batched solve (CUDA events around the graph launch) */
+double monolis_b200_batch_last_seconds(monolis_b200_batch* batch);
+
 /* ---- allocation-free inner product ----
  * No counterpart in the reference library.
  * *d_sum = sum_i d_x[i]*d_y[i] for device vectors of length n, enqueued on

@@ -168,6 +168,20 @@ _PRODUCT = {
     "monolis_b200_device_element_gradient_R": (C.c_int, [_MP, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                          C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                                          C.c_double, C.c_void_p]),
+    "monolis_b200_batch_create": (C.c_int, [C.POINTER(C.c_void_p)]),
+    "monolis_b200_batch_destroy": (None, [C.c_void_p]),
+    "monolis_b200_batch_add_system": (C.c_int, [C.c_void_p, _MP]),
+    "monolis_b200_batch_add_csr": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _ip, _ip, _dp]),
+    "monolis_b200_batch_prepare": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "monolis_b200_batch_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_longlong]),
+    "monolis_b200_batch_get_config": (C.c_int, [C.c_void_p, _ip, _ip, C.POINTER(C.c_longlong)]),
+    "monolis_b200_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _ip, C.POINTER(C.c_longlong), _dp]),
+    "monolis_b200_batch_solve_R": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int,
+                                             C.c_int, _ip, _dp, _ip]),
+    "monolis_b200_batch_info": (C.c_int, [C.c_void_p, _ip, C.POINTER(C.c_longlong)]),
+    "monolis_b200_batch_device_vectors": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "monolis_b200_batch_device_solve_R": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, _ip, _dp, _ip]),
+    "monolis_b200_batch_last_seconds": (C.c_double, [C.c_void_p]),
 }
 
 _ORACLE_EXTRA = {
@@ -493,6 +507,106 @@ class Monolis:
         if rc:
             raise RuntimeError("device_info: matrix not prepared")
         return nz.value, pad.value, ns.value
+
+
+class Batch:
+    """monolis_b200_batch_*: independent systems solved together by CG in one
+    persistent kernel."""
+
+    def __init__(self, lib: MonolisLib):
+        self.lib = lib
+        self.h = C.c_void_p()
+        _check(lib.monolis_b200_batch_create(C.byref(self.h)), "batch_create")
+        self.sizes = []
+        self.ndof = None
+
+    def add_system(self, m: "Monolis"):
+        _check(self.lib.monolis_b200_batch_add_system(self.h, m.p), "batch_add_system")
+        self.sizes.append(m.N * m.NDOF)
+        self.ndof = m.NDOF
+
+    def add_csr(self, n, ndof, index, item, val):
+        index = np.ascontiguousarray(index, dtype=np.int32)
+        item = np.ascontiguousarray(item, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        _check(self.lib.monolis_b200_batch_add_csr(self.h, n, ndof, _iptr(index), _iptr(item), _dptr(val)),
+               "batch_add_csr")
+        self.sizes.append(n * ndof)
+        self.ndof = ndof
+
+    def prepare(self, precond=1, autotune=True):
+        _check(self.lib.monolis_b200_batch_prepare(self.h, precond, int(autotune)), "batch_prepare")
+
+    def set_config(self, cluster, threads, split_rows):
+        _check(self.lib.monolis_b200_batch_set_config(self.h, cluster, threads, split_rows), "batch_set_config")
+
+    def config(self):
+        c, t, sp = C.c_int(), C.c_int(), C.c_longlong()
+        _check(self.lib.monolis_b200_batch_get_config(self.h, C.byref(c), C.byref(t), C.byref(sp)), "batch_config")
+        return c.value, t.value, sp.value
+
+    def autotune(self, iters=30, cap=64):
+        n = C.c_int(cap)
+        cl = (C.c_int * cap)()
+        th = (C.c_int * cap)()
+        sp = (C.c_longlong * cap)()
+        sec = (C.c_double * cap)()
+        _check(self.lib.monolis_b200_batch_autotune(self.h, iters, C.byref(n), cl, th, sp, sec), "batch_autotune")
+        return [(cl[i], th[i], sp[i], sec[i]) for i in range(min(n.value, cap))]
+
+    def solve(self, bs, tol=1e-8, max_iter=10000, refine=True):
+        """Host right-hand sides (list of arrays) -> (xs, iters, resid, status)."""
+        ns = len(self.sizes)
+        bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+        xs = [np.zeros(n) for n in self.sizes]
+        bp = (_dp * ns)(*[_dptr(b) for b in bs])
+        xp = (_dp * ns)(*[_dptr(x) for x in xs])
+        it = np.zeros(ns, dtype=np.int32)
+        res = np.zeros(ns)
+        st = np.zeros(ns, dtype=np.int32)
+        _check(self.lib.monolis_b200_batch_solve_R(self.h, bp, xp, tol, max_iter, int(refine), _iptr(it), _dptr(res),
+                                                   _iptr(st)), "batch_solve")
+        return xs, it, res, st
+
+    def offsets(self):
+        n = C.c_int()
+        _check(self.lib.monolis_b200_batch_info(self.h, C.byref(n), None), "batch_info")
+        off = (C.c_longlong * n.value)()
+        _check(self.lib.monolis_b200_batch_info(self.h, C.byref(n), off), "batch_info")
+        return np.array(off[:], dtype=np.int64)
+
+    def device_vectors(self):
+        db, dx = C.c_void_p(), C.c_void_p()
+        _check(self.lib.monolis_b200_batch_device_vectors(self.h, C.byref(db), C.byref(dx)), "batch_device_vectors")
+        return db.value, dx.value
+
+    def device_solve(self, tol=1e-8, max_iter=10000, refine=True):
+        ns = len(self.sizes)
+        it = np.zeros(ns, dtype=np.int32)
+        res = np.zeros(ns)
+        st = np.zeros(ns, dtype=np.int32)
+        _check(self.lib.monolis_b200_batch_device_solve_R(self.h, tol, max_iter, int(refine), _iptr(it), _dptr(res),
+                                                          _iptr(st)), "batch_device_solve")
+        return it, res, st
+
+    def last_seconds(self):
+        return self.lib.monolis_b200_batch_last_seconds(self.h)
+
+    def destroy(self):
+        if self.h:
+            self.lib.monolis_b200_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+def _check(rc, what):
+    if rc:
+        raise RuntimeError(f"{what} failed: {STATUS_NAMES.get(rc, rc)}")
 
 
 def stream_handle(lib: MonolisLib) -> int:

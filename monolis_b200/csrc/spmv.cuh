@@ -10,6 +10,15 @@
 
 namespace mb {
 
+// Gather of the multiplied vector. Kernels that read a vector written by
+// other blocks of the same launch (persistent kernels, between barriers)
+// must not use the non-coherent read-only path: kCoherent reads through L2.
+template <bool kCoherent, class T>
+__device__ __forceinline__ T ldx(const T* p) {
+  if constexpr (kCoherent) return __ldcg(p);
+  else return __ldg(p);
+}
+
 template <class V>
 struct SellView {
   const int* __restrict__ rowptr;
@@ -31,7 +40,7 @@ inline SellView<double> view_of<double>(const SellMatrix& m) {
 // (src/linalg/matvec.f90:805-823); the FP64 instantiation keeps exactly that
 // sequence of roundings. U slots are loaded before any is consumed so that
 // each thread keeps U*(B*B + 1) independent loads in flight.
-template <int B, int U, class V, class T>
+template <int B, int U, class V, class T, bool kCoherent = false>
 __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restrict__ x, int row, T (&y)[B]) {
   constexpr int B2 = B * B;
   const int lane = row & (kSlice - 1);
@@ -55,7 +64,7 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
     for (int u = 0; u < U; u++) {
       T xs[B];
 #pragma unroll
-      for (int l = 0; l < B; l++) xs[l] = __ldg(x + (long long)j[u] * B + l);
+      for (int l = 0; l < B; l++) xs[l] = ldx<kCoherent>(x + (long long)j[u] * B + l);
 #pragma unroll
       for (int r = 0; r < B; r++)
 #pragma unroll
@@ -69,7 +78,7 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
     for (int e = 0; e < B2; e++) a[e] = ld_stream(v + ((long long)k * B2 + e) * kSlice);
     T xs[B];
 #pragma unroll
-    for (int l = 0; l < B; l++) xs[l] = __ldg(x + (long long)jj * B + l);
+    for (int l = 0; l < B; l++) xs[l] = ldx<kCoherent>(x + (long long)jj * B + l);
 #pragma unroll
     for (int r = 0; r < B; r++)
 #pragma unroll
@@ -95,7 +104,7 @@ __device__ __forceinline__ int2 ld_stream2(const int2* p) { return __ldcs(p); }
 // y0/y1 = (A x) of rows 2t and 2t+1 in FP32 (fused multiply-add). Slots past
 // a row's length hold zero values and a valid column, so both rows run to the
 // longer length.
-template <int B, int U>
+template <int B, int U, bool kCoherent = false>
 __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
                                           float (&y1)[B]) {
   constexpr int B2 = B * B;
@@ -124,8 +133,8 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
       float x0[B], x1[B];
 #pragma unroll
       for (int l = 0; l < B; l++) {
-        x0[l] = __ldg(x + (long long)j[u].x * B + l);
-        x1[l] = __ldg(x + (long long)j[u].y * B + l);
+        x0[l] = ldx<kCoherent>(x + (long long)j[u].x * B + l);
+        x1[l] = ldx<kCoherent>(x + (long long)j[u].y * B + l);
       }
 #pragma unroll
       for (int r = 0; r < B; r++)
@@ -144,8 +153,8 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
     float x0[B], x1[B];
 #pragma unroll
     for (int l = 0; l < B; l++) {
-      x0[l] = __ldg(x + (long long)jj.x * B + l);
-      x1[l] = __ldg(x + (long long)jj.y * B + l);
+      x0[l] = ldx<kCoherent>(x + (long long)jj.x * B + l);
+      x1[l] = ldx<kCoherent>(x + (long long)jj.y * B + l);
     }
 #pragma unroll
     for (int r = 0; r < B; r++)

@@ -236,6 +236,53 @@ def smooth_target(n: int, seed: int = 5) -> np.ndarray:
     return np.ascontiguousarray(out.reshape(-1))
 
 
+def fv_diffusion_csr(side: int, seed: int):
+    """Cell-centred finite-volume diffusion on a side^3 cube of unit cells
+    (7-point stencil): per-cell conductivity kappa ~ LogNormal(0, 1), face
+    transmissibility the harmonic mean 2 k_i k_j / (k_i + k_j), zero Dirichlet
+    outside (boundary face 2 k_i). Returns the block CSR (0-based offsets and
+    columns, ascending columns, ndof 1): (index, item, val, kappa)."""
+    n = side ** 3
+    kappa = np.exp(normal(seed, n, 0.0, 1.0))
+    c = np.arange(n, dtype=np.int64)
+    ix, iy, iz = c % side, (c // side) % side, c // (side * side)
+    offs = [-side * side, -side, -1, 0, 1, side, side * side]
+    coord = [iz, iy, ix, None, ix, iy, iz]
+    cols = np.full((n, 7), -1, dtype=np.int64)
+    vals = np.zeros((n, 7))
+    diag = np.zeros(n)
+    for k, (o, q) in enumerate(zip(offs, coord)):
+        if o == 0:
+            continue
+        ok = (q > 0) if o < 0 else (q < side - 1)
+        j = c + o
+        t = np.zeros(n)
+        kj = kappa[np.where(ok, j, c)]
+        t_int = 2.0 * kappa * kj / (kappa + kj)
+        t = np.where(ok, t_int, 2.0 * kappa)
+        diag += t
+        cols[ok, k] = j[ok]
+        vals[ok, k] = -t_int[ok]
+    cols[:, 3] = c
+    vals[:, 3] = diag
+    valid = cols >= 0
+    index = np.zeros(n + 1, dtype=np.int32)
+    index[1:] = np.cumsum(valid.sum(axis=1))
+    return index, cols[valid].astype(np.int32), np.ascontiguousarray(vals[valid]), kappa
+
+
+def batch_sides(count: int = 512, seed: int = 4, lo: float = 10.0, hi: float = 60.0) -> np.ndarray:
+    """Side lengths round(exp(U(ln lo, ln hi))) of the batched workload."""
+    u = uniform(seed, count)
+    return np.rint(np.exp(np.log(lo) + u * (np.log(hi) - np.log(lo)))).astype(np.int64)
+
+
+def csr_matvec(index, item, val, x):
+    """y = A x for a 0-based scalar CSR (numpy, FP64)."""
+    rows = np.repeat(np.arange(len(index) - 1), np.diff(index))
+    return np.bincount(rows, weights=val * x[item], minlength=len(index) - 1)
+
+
 def spmv_bytes(nz: int, n: int, ndof: int, value_bytes: int) -> int:
     """Algorithmic bytes of one block SpMV: every value and column id read
     once, the row offsets once, x read once and y written once."""
