@@ -201,6 +201,87 @@ def workload_c3(lib, args, peak):
                         f"rel.res 1e-8, FP64 vs FP32-inner/FP64-refined", "by_peclet": out}
 
 
+def fp64_one_by_one(lib, systems, bs, tol):
+    """The plain FP64 GPU CG (monolis_b200_device_solve_R) on each system in
+    turn, device-resident b and x; returns summed device seconds, iterations."""
+    import torch
+    stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+    total, iters = 0.0, []
+    for (ix, it, v, _), b in zip(systems, bs):
+        m = api.Monolis(lib)
+        n = len(ix) - 1
+        m.set_matrix_BCSR(n, n, 1, len(it), v, ix, it)
+        m.quiet()
+        m.set_error_abort(False)
+        m.set_method(api.ITER_CG)
+        m.set_precond(api.PREC_DIAG)
+        m.set_tolerance(tol)
+        m.set_maxiter(20000)
+        m.set_matrix_cache(True)
+        m.device_prepare()
+        d_b = torch.from_numpy(b).cuda()
+        d_x = torch.zeros_like(d_b)
+        total += device_solve_timed(m, stream, d_b, d_x)
+        iters.append(m.get_converge_iter())
+        m.finalize()
+    return total, iters
+
+
+def batch_run(lib, systems, bs, label):
+    """Stack the systems into one batch, autotune, solve FP32-refined to 1e-8
+    and FP32-only to 1e-6; check every system's FP64 residual in numpy."""
+    batch = api.Batch(lib)
+    for ix, it, v, _ in systems:
+        batch.add_csr(len(ix) - 1, 1, ix, it, v)
+    t0 = time.perf_counter()
+    batch.prepare(precond=api.PREC_DIAG, autotune=True)
+    t_prep = time.perf_counter() - t0
+    cands = batch.autotune(iters=30)
+    cfg = batch.config()
+    out = {"systems": len(systems), "unknowns": int(sum(len(b) for b in bs)), "prepare_s": t_prep,
+           "config": {"cluster": cfg[0], "threads": cfg[1], "split_rows": cfg[2]},
+           "autotune": [{"cluster": c[0], "threads": c[1], "split_rows": c[2], "s": c[3]} for c in cands]}
+    for name, tol, refine in (("refined_1e-8", 1e-8, True), ("fp32_1e-6", 1e-6, False)):
+        xs, its, res, st = batch.solve(bs, tol=tol, max_iter=20000, refine=refine)  # warm-up; uploads b
+        t_e2e0 = time.perf_counter()
+        xs, its, res, st = batch.solve(bs, tol=tol, max_iter=20000, refine=refine)
+        t_e2e = time.perf_counter() - t_e2e0
+        its2, res2, st2 = batch.device_solve(tol=tol, max_iter=20000, refine=refine)
+        t_dev = batch.last_seconds()
+        true = [float(np.linalg.norm(b - problems.csr_matvec(ix, it, v, x)) / np.linalg.norm(b))
+                for (ix, it, v, _), x, b in zip(systems, xs, bs)]
+        out[name] = {"s": t_dev, "e2e_s": t_e2e, "all_converged": bool(np.all(st2 == 0)),
+                     "max_true_rel_residual": max(true), "iterations_max": int(its2.max()),
+                     "iterations_mean": float(its2.mean())}
+    batch.destroy()
+    log(f"[rank 0] batch {label}: {json.dumps({k: out[k] for k in out if k != 'autotune'})[:300]}")
+    return out
+
+
+def workload_c4(lib, args):
+    """512 independent FV diffusion systems (side log-uniform in [10, 60]) in
+    one batch, and one 96^3 system with 32 right-hand sides; each against the
+    plain FP64 GPU CG solving the systems one by one."""
+    sides = problems.batch_sides(args.c4_count)
+    systems = [problems.fv_diffusion_csr(int(s), 4000 + i) for i, s in enumerate(sides)]
+    bs = [problems.uniform(5000 + i, int(s) ** 3) for i, s in enumerate(sides)]
+    res = {"workload": f"{len(sides)} cell-centred FV diffusion systems, side round(exp(U(ln10, ln60))), "
+                       f"log-normal kappa, CG + DIAG; FP32 batched (1e-6) and FP32-refined (1e-8) vs FP64 GPU "
+                       f"CG one system at a time (1e-8)"}
+    res["many_systems"] = batch_run(lib, systems, bs, "many systems")
+    t64, it64 = fp64_one_by_one(lib, systems, bs, 1e-8)
+    res["many_systems"]["fp64_one_by_one_s"] = t64
+    res["many_systems"]["speedup_refined_vs_fp64"] = t64 / res["many_systems"]["refined_1e-8"]["s"]
+    # one 96^3 system with 32 right-hand sides: the batch holds 32 copies of the matrix
+    one = problems.fv_diffusion_csr(args.c4_rhs_side, 4999)
+    rhs = [problems.uniform(6000 + k, args.c4_rhs_side ** 3) for k in range(args.c4_rhs)]
+    res["many_rhs"] = batch_run(lib, [one] * args.c4_rhs, rhs, "many rhs")
+    t64r, _ = fp64_one_by_one(lib, [one] * args.c4_rhs, rhs, 1e-8)
+    res["many_rhs"]["fp64_one_by_one_s"] = t64r
+    res["many_rhs"]["speedup_refined_vs_fp64"] = t64r / res["many_rhs"]["refined_1e-8"]["s"]
+    return res
+
+
 def workload_c5(lib, args):
     """Adjoint gradient of L = 1/2 ||x - x_target||^2 for 3D Q1 diffusion with
     per-element log-normal conductivity (128^3 nodes): forward CG to 1e-10,
@@ -357,7 +438,11 @@ def main():
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workloads", default="c3,c5", help="secondary workloads to run after the headline (c3,c5 or none)")
+    ap.add_argument("--workloads", default="c3,c4,c5",
+                    help="secondary workloads to run after the headline (any of c3,c4,c5, or none)")
+    ap.add_argument("--c4-count", type=int, default=512)
+    ap.add_argument("--c4-rhs-side", type=int, default=96)
+    ap.add_argument("--c4-rhs", type=int, default=32)
     ap.add_argument("--c3-n", type=int, default=256)
     ap.add_argument("--c3-peclet", type=float, nargs="+", default=[0.5, 5.0, 50.0])
     ap.add_argument("--c5-n", type=int, default=128)
@@ -548,6 +633,8 @@ def main():
                     workloads["c3"] = workload_c3(lib, args, peak)
                 elif w == "c5":
                     workloads["c5"] = workload_c5(lib, args)
+                elif w == "c4":
+                    workloads["c4"] = workload_c4(lib, args)
             except Exception as e:  # report, do not hide
                 workloads[w] = {"failed": repr(e)}
             log(f"[rank 0] workload {w}: {json.dumps(workloads[w])[:400]}")
