@@ -191,6 +191,20 @@ int  monolis_b200_batch_device_solve_R(monolis_b200_batch* batch, double tol, in
 /* device seconds of the last batched solve (CUDA events around the graph launch) */
 double monolis_b200_batch_last_seconds(monolis_b200_batch* batch);
 
+/* ---- many right-hand sides on one matrix ----
+ * No counterpart in the reference library (one right-hand side per solve).
+ * Solves A X_k = B_k for k < n_rhs with CG and the struct's preconditioner
+ * (None or Diag), tolerance and max_iter; B_k and X_k are stored one after
+ * another (B + k*N*ndof, like B(:,k)). Up to 32 right-hand sides share each
+ * pass over the matrix (more are done 32 at a time), in one persistent
+ * kernel; each converges on its own. PRECISION MIXED: FP32 loop with FP64
+ * reliable updates (tol on the FP64 residual); FP64: the loop in double.
+ * iter, resid (relative FP64 residual), status: per right-hand side. */
+int monolis_b200_solve_multi_R(MONOLIS* mat, MONOLIS_COM* com, int n_rhs, double* B, double* X, int* iter,
+                               double* resid, int* status);
+int monolis_b200_device_solve_multi_R(MONOLIS* mat, int n_rhs, const double* d_B, double* d_X, int* iter,
+                                      double* resid, int* status);
+
 /* ---- allocation-free inner product ----
  * No counterpart in the reference library.
  * *d_sum = sum_i d_x[i]*d_y[i] for device vectors of length n, enqueued on

@@ -182,6 +182,8 @@ _PRODUCT = {
     "monolis_b200_batch_device_vectors": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "monolis_b200_batch_device_solve_R": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, _ip, _dp, _ip]),
     "monolis_b200_batch_last_seconds": (C.c_double, [C.c_void_p]),
+    "monolis_b200_solve_multi_R": (C.c_int, [_MP, _CP, C.c_int, _dp, _dp, _ip, _dp, _ip]),
+    "monolis_b200_device_solve_multi_R": (C.c_int, [_MP, C.c_int, C.c_void_p, C.c_void_p, _ip, _dp, _ip]),
 }
 
 _ORACLE_EXTRA = {
@@ -483,6 +485,20 @@ class Monolis:
         if rc:
             raise RuntimeError(f"element_gradient failed: {STATUS_NAMES.get(rc, rc)}")
         return grad
+
+    def solve_multi(self, B):
+        """monolis_b200_solve_multi_R: B is (n_rhs, N*ndof); returns (X, iter, resid, status)."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        nr = B.shape[0]
+        X = np.zeros_like(B)
+        it = np.zeros(nr, dtype=np.int32)
+        res = np.zeros(nr)
+        st = np.zeros(nr, dtype=np.int32)
+        rc = self.lib.monolis_b200_solve_multi_R(self.p, C.pointer(self.com), nr, _dptr(B), _dptr(X), _iptr(it),
+                                                 _dptr(res), _iptr(st))
+        if rc:
+            raise RuntimeError(f"solve_multi failed: {STATUS_NAMES.get(rc, rc)}")
+        return X, it, res, st
 
     # ---- device entry points (product only) ----
     def device_prepare(self):

@@ -245,6 +245,7 @@ struct DevState {
   mb::SellMatrix A;
   mb::SellMatrix AT;  // A^T, built on demand from A's device CSR and the CSC arrays
   long long build_id = 0, at_build_id = -1;
+  mb::MultiState* multi = nullptr;  // many-right-hand-side solver buffers
   mb::Scratch sc;
   double* d_b = nullptr;
   double* d_x = nullptr;
@@ -305,6 +306,7 @@ void state_release(const MONOLIS* m) {
     cudaStreamSynchronize(c.stream);
     mb::sell_free(s->A);
     mb::sell_free(s->AT);
+    mb::multi_free(s->multi);
     mb::scratch_free(s->sc);
     cudaFree(s->d_b);
     cudaFree(s->d_x);
@@ -1003,6 +1005,57 @@ int monolis_b200_device_solve_transpose_R(MONOLIS* m, const double* d_b, double*
   if (rc) return rc;
   print_summary(m);
   return m->prm.Iarray[MONOLIS_PRM_I_IERR];
+}
+
+int monolis_b200_device_solve_multi_R(MONOLIS* m, int n_rhs, const double* d_B, double* d_X, int* iter,
+                                      double* resid, int* status) {
+  int* I = m->prm.Iarray;
+  const int mth = I[MONOLIS_PRM_I_METHOD], pc = I[MONOLIS_PRM_I_PRECOND];
+  if (mth != MONOLIS_ITER_CG || (pc != MONOLIS_PREC_NONE && pc != MONOLIS_PREC_DIAG) || n_rhs < 1) {
+    fprintf(stderr, "** monolis_b200: the many-right-hand-side solver runs CG with None or Diag\n");
+    return MONOLIS_B200_BAD_INPUT;
+  }
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  const bool mixed = I[MONOLIS_B200_PRM_I_PRECISION] == 1;
+  int rc = prepare(m, s, pc == MONOLIS_PREC_DIAG, mixed, nullptr);
+  if (rc) return rc;
+  if (!s->multi) s->multi = mb::multi_new();
+  const double t0 = now_sec();
+  rc = mb::multi_solve(s->A, *s->multi, s->build_id, n_rhs, d_B, d_X, mixed ? 1 : 0, pc == MONOLIS_PREC_DIAG ? 1 : 0,
+                       m->prm.Rarray[MONOLIS_PRM_R_TOL], I[MONOLIS_PRM_I_MAX_ITER],
+                       m->prm.Rarray[MONOLIS_B200_PRM_R_REFRESH_DELTA], iter, resid, status, ctx().stream);
+  m->prm.Rarray[MONOLIS_B200_PRM_R_TIME_LOOP] = now_sec() - t0;
+  I[MONOLIS_PRM_I_IERR] = rc;
+  return rc;
+}
+
+int monolis_b200_solve_multi_R(MONOLIS* m, MONOLIS_COM* com, int n_rhs, double* B, double* X, int* iter,
+                               double* resid, int* status) {
+  if ((com && com->comm_size > 1) || n_rhs < 1 || !B || !X) return MONOLIS_B200_BAD_INPUT;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  }
+  const size_t n = (size_t)m->mat.N * m->mat.NDOF * n_rhs;
+  cudaStream_t st = ctx().stream;
+  double *d_B = nullptr, *d_X = nullptr;
+  MB_API_CUDA(cudaMalloc((void**)&d_B, n * sizeof(double)));
+  if (cudaMalloc((void**)&d_X, n * sizeof(double)) != cudaSuccess) {
+    cudaFree(d_B);
+    return MONOLIS_B200_CUDA_ERROR;
+  }
+  int rc = MONOLIS_B200_OK;
+  if (cudaMemcpyAsync(d_B, B, n * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
+    rc = MONOLIS_B200_CUDA_ERROR;
+  if (!rc) rc = monolis_b200_device_solve_multi_R(m, n_rhs, d_B, d_X, iter, resid, status);
+  if (!rc && cudaMemcpyAsync(X, d_X, n * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    rc = MONOLIS_B200_CUDA_ERROR;
+  if (cudaStreamSynchronize(st) != cudaSuccess) rc = MONOLIS_B200_CUDA_ERROR;
+  cudaFree(d_B);
+  cudaFree(d_X);
+  return rc;
 }
 
 int monolis_b200_device_matvec_transpose_R(MONOLIS* m, const double* d_x, double* d_y) {

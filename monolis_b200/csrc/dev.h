@@ -144,6 +144,17 @@ struct SolveResult {
 int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double* d_b, double* d_x,
                  SolveResult& res, double* h_hist, cudaStream_t s);
 
+// ---- many right-hand sides on one matrix (multi.cu) ----
+struct MultiState;
+MultiState* multi_new();
+void multi_free(MultiState* ms);
+// n_rhs systems A X_k = B_k with B_k at d_B + k*N*ndof (device); precision 1:
+// FP32 loop with FP64 refresh, 0: FP64. build_id identifies the device
+// matrix contents (the FP32 CSR copy is rebuilt when it changes).
+int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, const double* d_B, double* d_X,
+                int precision, int prec, double tol, int max_iter, double delta, int* iter, double* resid,
+                int* status, cudaStream_t s);
+
 int scratch_ensure(Scratch& sc, size_t hist_len);
 void scratch_free(Scratch& sc);
 
