@@ -34,11 +34,20 @@ namespace {
 
 constexpr int kMultiK = 32;
 constexpr int kMultiThreads = 256;
-constexpr unsigned long long kSpinLimit = 1ull << 24;  // polls of ~100 ns: ~2 s
+constexpr unsigned long long kSpinLimit = 1ull << 22;  // polls (an L2 round trip + 32 ns each): seconds
+
+constexpr int kBarrierGroup = 32;  // blocks per first-level group of the barrier
+constexpr int kMaxGroups = 128;
+
+constexpr int kLine = 32;  // words per 128-byte line: every counter and flag gets its own
 
 struct MultiCtl {
-  unsigned int count, gen;
-  int err, all_done, any_refresh, it;
+  alignas(128) unsigned int count;  // groups finished (global arrival)
+  alignas(128) unsigned int gen;    // global release generation
+  alignas(128) int err;
+  int all_done, any_refresh, it;
+  alignas(128) unsigned int gcount[kMaxGroups * kLine];  // blocks arrived, per group
+  alignas(128) unsigned int grel[kMaxGroups * kLine];    // release generation, per group
   double rho[kMultiK], rho1[kMultiK], alpha[kMultiK], beta[kMultiK], B2[kMultiK], rmax[kMultiK], resid[kMultiK];
   int iter[kMultiK], done[kMultiK], status[kMultiK], refresh[kMultiK], fold[kMultiK], nref[kMultiK];
 };
@@ -68,37 +77,87 @@ __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Grid barrier of a cooperative launch. The last block to arrive runs
-// `last` (with all its threads) before releasing the others. Returns false
-// once any block has given up waiting.
+// Grid barrier of a cooperative launch, with an optional reduction of the
+// per-block partial sums (2 x 32 doubles per block, partials[block][64]).
+// Blocks arrive in groups of kBarrierGroup: the last block of a group sums
+// the group's partials in block order (group sums after the block partials),
+// the last group finisher sums the group sums in group order into tot and
+// runs `last` (with all its threads) before releasing everyone. Each block
+// adds at most one group's worth of values, so the barrier's tail stays short.
+// Waits are bounded; returns false once any block has given up.
 template <class F>
-__device__ bool grid_sync(MultiCtl* c, F&& last) {
-  __shared__ unsigned int s_gen;
-  __shared__ int s_last, s_ok;
+__device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*tot)[kMultiK], F&& last) {
+  __shared__ unsigned int s_grel, s_gen;
+  __shared__ int s_role, s_ok;  // 0: wait for the group, 1: group finisher, 2: last block
+  const unsigned int G = gridDim.x, g = blockIdx.x / kBarrierGroup;
+  const unsigned int ngroups = (G + kBarrierGroup - 1) / kBarrierGroup;
+  const unsigned int g0 = g * kBarrierGroup, gsize = min((unsigned int)kBarrierGroup, G - g0);
+  unsigned int* gcount = c->gcount + g * kLine;
+  unsigned int* grel = c->grel + g * kLine;
+  double* gpart = partials + (size_t)G * 2 * kMultiK;
   __syncthreads();
   if (threadIdx.x == 0) {
+    s_grel = ld_acquire(grel);
     s_gen = ld_acquire(&c->gen);
     __threadfence();
-    s_last = atomicAdd(&c->count, 1u) == gridDim.x - 1;
+    s_role = atomicAdd(gcount, 1u) == gsize - 1 ? 1 : 0;
   }
   __syncthreads();
-  if (s_last) {
+  if (s_role == 1) {
     __threadfence();
-    last();
+    if (reduce && threadIdx.x < 2 * kMultiK) {
+      double s = 0.0;
+#pragma unroll 8
+      for (unsigned int b = 0; b < gsize; b++) s += __ldcg(partials + (size_t)(g0 + b) * 2 * kMultiK + threadIdx.x);
+      gpart[(size_t)g * 2 * kMultiK + threadIdx.x] = s;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
-      c->count = 0u;
+      *gcount = 0u;
       __threadfence();
-      st_release(&c->gen, s_gen + 1u);
+      if (atomicAdd(&c->count, 1u) == ngroups - 1) s_role = 2;
     }
+    __syncthreads();
+    if (s_role == 2) {
+      __threadfence();
+      if (reduce) {
+        if (threadIdx.x < 2 * kMultiK) {
+          double t = 0.0;
+#pragma unroll 8
+          for (unsigned int q = 0; q < ngroups; q++) t += __ldcg(gpart + (size_t)q * 2 * kMultiK + threadIdx.x);
+          tot[threadIdx.x >> 5][threadIdx.x & 31] = t;
+        }
+        __syncthreads();
+      }
+      last();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        c->count = 0u;
+        __threadfence();
+        st_release(&c->gen, s_gen + 1u);
+      }
+    } else if (threadIdx.x == 0) {
+      // group finisher: wait for the global release (at most ngroups pollers)
+      unsigned long long n = 0;
+      while (ld_acquire(&c->gen) == s_gen) {
+        if (++n > kSpinLimit) {
+          atomicExch(&c->err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+      __threadfence();
+    }
+    if (threadIdx.x == 0) st_release(grel, s_grel + 1u);  // release this group
   } else if (threadIdx.x == 0) {
+    // wait for this group's release (at most kBarrierGroup pollers per line)
     unsigned long long n = 0;
-    while (ld_acquire(&c->gen) == s_gen) {
+    while (ld_acquire(grel) == s_grel) {
       if (++n > kSpinLimit) {
         atomicExch(&c->err, 1);
         break;
       }
-      __nanosleep(100);
+      __nanosleep(32);
     }
     __threadfence();
   }
@@ -121,23 +180,6 @@ __device__ __forceinline__ void write_partials(double v0, double v1, double (*s_
   }
 }
 
-// In the last block: tot[which][k] = sum over blocks of the partials, in
-// block order split over the block's threads, then combined in fixed order.
-__device__ __forceinline__ void sum_partials(const double* partials, double (*s_part)[2 * kMultiK],
-                                             double (*tot)[kMultiK]) {
-  const int pair = threadIdx.x & (2 * kMultiK - 1), sub = threadIdx.x >> 6, nsub = blockDim.x >> 6;
-  double s = 0.0;
-  for (unsigned int b = sub; b < gridDim.x; b += nsub) s += __ldcg(partials + (size_t)b * 2 * kMultiK + pair);
-  s_part[sub][pair] = s;
-  __syncthreads();
-  if (threadIdx.x < 2 * kMultiK) {
-    double t = 0.0;
-    for (int i = 0; i < nsub; i++) t += s_part[i][threadIdx.x];
-    tot[threadIdx.x >> 5][threadIdx.x & 31] = t;
-  }
-  __syncthreads();
-}
-
 template <class T>
 __device__ __forceinline__ T fmat(T a, T b, T c);
 template <>
@@ -145,11 +187,28 @@ __device__ __forceinline__ float fmat<float>(float a, float b, float c) { return
 template <>
 __device__ __forceinline__ double fmat<double>(double a, double b, double c) { return fma(a, b, c); }
 
+// Small blocks: at most 64 registers, so that 4 blocks (32 warps) per SM
+// keep enough loads in flight for HBM bandwidth.
 template <int B, class T>
-__global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs<T> a) {
+__global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel(const MultiArgs<T> a) {
   constexpr int B2 = B * B;
+  constexpr int kCh = B == 1 ? 8 : (B == 2 ? 4 : (B == 3 ? 2 : 1));  // row entries gathered together
+  constexpr int kRows = B == 1 ? 4 : (B <= 3 ? 2 : 1);                // rows per step of the update
+  constexpr int kChR = kCh > 1 ? kCh / 2 : 1;  // the (rare) FP64 refresh: fewer registers
+  // the arrays never alias: tell the compiler, so that loads of the next
+  // rows may move above the stores of the current ones
+  const int* __restrict__ rowptr = a.rowptr;
+  const int* __restrict__ colv = a.col;
+  const T* __restrict__ val = a.val;
+  const double* __restrict__ val64 = a.val64;
+  const T* __restrict__ alu = a.alu;
+  const double* __restrict__ bv = a.b;
+  double* __restrict__ xv = a.x;
+  T* __restrict__ yv_ = a.y;
+  T* __restrict__ rv_ = a.r;
+  T* __restrict__ zv = a.z;
+  T* __restrict__ qv_ = a.q;
   __shared__ double s_red[kMultiThreads / 32][2][kMultiK];
-  __shared__ double s_part[kMultiThreads / 64][2 * kMultiK];
   __shared__ double s_tot[2][kMultiK];
   __shared__ int s_flag[2];
   const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -169,8 +228,8 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
     if (act)
 #pragma unroll
       for (int cc = 0; cc < B; cc++) {
-        a.x[at(row, cc)] = 0.0;
-        a.y[at(row, cc)] = T(0);
+        xv[at(row, cc)] = 0.0;
+        yv_[at(row, cc)] = T(0);
       }
 
   // r = b - A (x + y) in FP64, z = M^-1 r, for the lanes with `mine` set
@@ -178,7 +237,7 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
   auto refresh = [&](bool mine) {
     double v0 = 0.0, v1 = 0.0;
     for (long long row = gw; row < a.N; row += W) {
-      const int k0 = a.rowptr[row], len = a.rowptr[row + 1] - k0;
+      const int k0 = rowptr[row], len = rowptr[row + 1] - k0;
       double ax[B];
 #pragma unroll
       for (int cc = 0; cc < B; cc++) ax[cc] = 0.0;
@@ -189,26 +248,35 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
 #pragma unroll
         for (int e = 0; e < B2; e++) vv[e] = 0.0;
         if (lane < m) {
-          cj = a.col[k0 + base + lane];
+          cj = colv[k0 + base + lane];
 #pragma unroll
-          for (int e = 0; e < B2; e++) vv[e] = a.val64[(long long)(k0 + base + lane) * B2 + e];
+          for (int e = 0; e < B2; e++) vv[e] = val64[(long long)(k0 + base + lane) * B2 + e];
         }
-        for (int t = 0; t < m; t++) {
-          const int j = __shfl_sync(0xffffffffu, cj, t);
-          double ae[B2];
+        for (int t0 = 0; t0 < m; t0 += kChR) {
+          int jj[kChR];
+          double ae[kChR][B2];
 #pragma unroll
-          for (int e = 0; e < B2; e++) ae[e] = __shfl_sync(0xffffffffu, vv[e], t);
+          for (int u = 0; u < kChR; u++) {
+            jj[u] = __shfl_sync(0xffffffffu, cj, (t0 + u) & 31);
+#pragma unroll
+            for (int e = 0; e < B2; e++) ae[u][e] = __shfl_sync(0xffffffffu, vv[e], (t0 + u) & 31);
+          }
           if (act && mine) {
-            double xs[B];
+            double xs[kChR][B];
 #pragma unroll
-            for (int l = 0; l < B; l++) {
-              const long long ij = ((long long)j * B + l) * K + k;
-              xs[l] = __ldcg(a.x + ij) + (double)__ldcg(a.y + ij);
-            }
+            for (int u = 0; u < kChR; u++)
 #pragma unroll
-            for (int rr = 0; rr < B; rr++)
+              for (int l = 0; l < B; l++) {
+                const long long ij = ((long long)jj[u] * B + l) * K + k;
+                xs[u][l] = __ldcg(xv + ij) + (double)__ldcg(yv_ + ij);
+              }
 #pragma unroll
-              for (int l = 0; l < B; l++) ax[rr] = fma(ae[rr * B + l], xs[l], ax[rr]);
+            for (int u = 0; u < kChR; u++)
+              if (t0 + u < m)
+#pragma unroll
+                for (int rr = 0; rr < B; rr++)
+#pragma unroll
+                  for (int l = 0; l < B; l++) ax[rr] = fma(ae[u][rr * B + l], xs[u][l], ax[rr]);
           }
         }
       }
@@ -216,16 +284,16 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
         T t[B], w[B];
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
-          const double rv = a.b[at(row, cc)] - ax[cc];
+          const double rv = bv[at(row, cc)] - ax[cc];
           v0 += rv * rv;
           t[cc] = (T)rv;
           w[cc] = t[cc];
-          a.r[at(row, cc)] = t[cc];
+          rv_[at(row, cc)] = t[cc];
         }
-        if (a.prec) diag_row<B, T>(a.alu, a.N, (int)row, w);
+        if (a.prec) diag_row<B, T>(alu, a.N, (int)row, w);
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
-          a.z[at(row, cc)] = w[cc];
+          zv[at(row, cc)] = w[cc];
           v1 += (double)t[cc] * (double)w[cc];
         }
       }
@@ -234,10 +302,9 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
   };
 
   // the whole grid has zeroed its x and y before any residual reads them
-  if (!grid_sync(c, [] {})) return;
+  if (!grid_sync(c, a.partials, false, s_tot, [] {})) return;
   refresh(true);
-  if (!grid_sync(c, [&] {
-        sum_partials(a.partials, s_part, s_tot);
+  if (!grid_sync(c, a.partials, true, s_tot, [&] {
         if (threadIdx.x < K) {
           const int kk = threadIdx.x;
           const double rr = s_tot[0][kk], rz = s_tot[1][kk];
@@ -272,7 +339,7 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
     // and the old P at the neighbours; <P,Q>
     double pq = 0.0;
     for (long long row = gw; row < a.N; row += W) {
-      const int k0 = a.rowptr[row], len = a.rowptr[row + 1] - k0;
+      const int k0 = rowptr[row], len = rowptr[row + 1] - k0;
       T acc[B];
 #pragma unroll
       for (int cc = 0; cc < B; cc++) acc[cc] = T(0);
@@ -283,27 +350,42 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
 #pragma unroll
         for (int e = 0; e < B2; e++) vv[e] = T(0);
         if (lane < m) {
-          cj = a.col[k0 + base + lane];
+          cj = colv[k0 + base + lane];
 #pragma unroll
-          for (int e = 0; e < B2; e++) vv[e] = a.val[(long long)(k0 + base + lane) * B2 + e];
+          for (int e = 0; e < B2; e++) vv[e] = val[(long long)(k0 + base + lane) * B2 + e];
         }
-        for (int t = 0; t < m; t++) {
-          const int j = __shfl_sync(0xffffffffu, cj, t);
-          T ae[B2];
+        // kCh entries at a time: all their gathers are issued before any is
+        // used (lanes past the row end hold column 0 and value 0)
+        for (int t0 = 0; t0 < m; t0 += kCh) {
+          int jj[kCh];
+          T ae[kCh][B2];
 #pragma unroll
-          for (int e = 0; e < B2; e++) ae[e] = __shfl_sync(0xffffffffu, vv[e], t);
+          for (int u = 0; u < kCh; u++) {
+            jj[u] = __shfl_sync(0xffffffffu, cj, (t0 + u) & 31);
+#pragma unroll
+            for (int e = 0; e < B2; e++) ae[u][e] = __shfl_sync(0xffffffffu, vv[e], (t0 + u) & 31);
+          }
           if (!done_k) {
-            T ps[B];
+            T zs[kCh][B], po[kCh][B];
 #pragma unroll
-            for (int l = 0; l < B; l++) {
-              const long long ij = ((long long)j * B + l) * K + k;
-              const T zj = __ldcg(a.z + ij);
-              ps[l] = first ? zj : fmat<T>(beta, __ldcg(pold + ij), zj);
+            for (int u = 0; u < kCh; u++)
+#pragma unroll
+              for (int l = 0; l < B; l++) {
+                const long long ij = ((long long)jj[u] * B + l) * K + k;
+                zs[u][l] = __ldcg(zv + ij);
+                po[u][l] = first ? T(0) : __ldcg(pold + ij);
+              }
+#pragma unroll
+            for (int u = 0; u < kCh; u++) {
+              if (t0 + u < m) {
+#pragma unroll
+                for (int l = 0; l < B; l++) {
+                  const T pl = first ? zs[u][l] : fmat<T>(beta, po[u][l], zs[u][l]);
+#pragma unroll
+                  for (int rr = 0; rr < B; rr++) acc[rr] = fmat<T>(ae[u][rr * B + l], pl, acc[rr]);
+                }
+              }
             }
-#pragma unroll
-            for (int rr = 0; rr < B; rr++)
-#pragma unroll
-              for (int l = 0; l < B; l++) acc[rr] = fmat<T>(ae[rr * B + l], ps[l], acc[rr]);
           }
         }
       }
@@ -311,21 +393,20 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
           const long long i = at(row, cc);
-          const T pv = first ? a.z[i] : fmat<T>(beta, pold[i], a.z[i]);
+          const T pv = first ? zv[i] : fmat<T>(beta, pold[i], zv[i]);
           pnew[i] = pv;
-          a.q[i] = acc[cc];
+          qv_[i] = acc[cc];
           pq += (double)pv * (double)acc[cc];
           if (fold) {
-            a.x[i] += (double)a.y[i];
-            a.y[i] = T(0);
+            xv[i] += (double)yv_[i];
+            yv_[i] = T(0);
           }
         }
       }
     }
     write_partials(pq, 0.0, s_red, a.partials);
-    if (!grid_sync(c, [&] {
-          sum_partials(a.partials, s_part, s_tot);
-          if (threadIdx.x < K && !vc->done[threadIdx.x]) {
+    if (!grid_sync(c, a.partials, true, s_tot, [&] {
+            if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
             const double w = s_tot[0][kk];
             vc->fold[kk] = 0;
@@ -343,30 +424,47 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
       const bool live = act && __ldcg(&c->done[k]) == 0;
       const T alpha = live ? (T)__ldcg(&c->alpha[k]) : T(0);
       double v0 = 0.0, v1 = 0.0;
-      for (long long row = gw; row < a.N; row += W) {
-        if (!live) continue;
-        T t[B], w[B];
+      // kRows rows per step: the loads of all of them are in flight together
+      for (long long row = gw; live && row < a.N; row += kRows * W) {
+        const int nr = (int)min((long long)kRows, (a.N - row + W - 1) / W);
+        T pv[kRows][B], qv[kRows][B], rv[kRows][B], yv[kRows][B];
 #pragma unroll
-        for (int cc = 0; cc < B; cc++) {
-          const long long i = at(row, cc);
-          a.y[i] = fmat<T>(alpha, pnew[i], a.y[i]);
-          t[cc] = fmat<T>(-alpha, a.q[i], a.r[i]);
-          a.r[i] = t[cc];
-          w[cc] = t[cc];
-        }
-        if (a.prec) diag_row<B, T>(a.alu, a.N, (int)row, w);
+        for (int h = 0; h < kRows; h++)
+          if (h < nr)
 #pragma unroll
-        for (int cc = 0; cc < B; cc++) {
-          a.z[at(row, cc)] = w[cc];
-          v0 += (double)t[cc] * (double)t[cc];
-          v1 += (double)t[cc] * (double)w[cc];
+            for (int cc = 0; cc < B; cc++) {
+              const long long i = at(row + h * W, cc);
+              pv[h][cc] = pnew[i];
+              qv[h][cc] = qv_[i];
+              rv[h][cc] = rv_[i];
+              yv[h][cc] = yv_[i];
+            }
+#pragma unroll
+        for (int h = 0; h < kRows; h++) {
+          if (h >= nr) break;
+          const long long rw = row + h * W;
+          T t[B], w[B];
+#pragma unroll
+          for (int cc = 0; cc < B; cc++) {
+            const long long i = at(rw, cc);
+            yv_[i] = fmat<T>(alpha, pv[h][cc], yv[h][cc]);
+            t[cc] = fmat<T>(-alpha, qv[h][cc], rv[h][cc]);
+            rv_[i] = t[cc];
+            w[cc] = t[cc];
+          }
+          if (a.prec) diag_row<B, T>(alu, a.N, (int)rw, w);
+#pragma unroll
+          for (int cc = 0; cc < B; cc++) {
+            zv[at(rw, cc)] = w[cc];
+            v0 += (double)t[cc] * (double)t[cc];
+            v1 += (double)t[cc] * (double)w[cc];
+          }
         }
       }
       write_partials(v0, v1, s_red, a.partials);
     }
-    if (!grid_sync(c, [&] {
-          sum_partials(a.partials, s_part, s_tot);
-          int any = 0;
+    if (!grid_sync(c, a.partials, true, s_tot, [&] {
+            int any = 0;
           if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
             const double rr = s_tot[0][kk], rz = s_tot[1][kk];
@@ -400,9 +498,8 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
     if (__ldcg(&c->any_refresh)) {
       const bool mine = act && __ldcg(&c->refresh[k]) != 0;
       refresh(mine);
-      if (!grid_sync(c, [&] {
-            sum_partials(a.partials, s_part, s_tot);
-            if (threadIdx.x < K && vc->refresh[threadIdx.x]) {
+      if (!grid_sync(c, a.partials, true, s_tot, [&] {
+                if (threadIdx.x < K && vc->refresh[threadIdx.x]) {
               const int kk = threadIdx.x;
               const double rr = s_tot[0][kk], rz = s_tot[1][kk];
               const double resid = sqrt(rr / vc->B2[kk]);
@@ -450,8 +547,8 @@ __global__ void __launch_bounds__(kMultiThreads) multi_cg_kernel(const MultiArgs
 #pragma unroll
       for (int cc = 0; cc < B; cc++) {
         const long long i = at(row, cc);
-        a.x[i] += (double)a.y[i];
-        a.y[i] = T(0);
+        xv[i] += (double)yv_[i];
+        yv_[i] = T(0);
       }
 }
 
@@ -499,7 +596,8 @@ int launch_multi(const MultiArgs<T>& args, cudaStream_t s) {
   MB_CUDA_OK(cudaGetDevice(&dev));
   MB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) return kBadInput;
-  const int grid = per_sm * sms;  // every block resident (cooperative launch)
+  // every block resident (cooperative launch), within the barrier's group table
+  const int grid = std::min(per_sm * sms, kMaxGroups * kBarrierGroup);
   MultiArgs<T> a = args;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
@@ -573,7 +671,8 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
   int dev = 0, sms = 0;
   MB_CUDA_OK(cudaGetDevice(&dev));
   MB_CUDA_OK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const size_t part = (size_t)sms * (2048 / kMultiThreads) * 2 * kMultiK;  // resident blocks x partials
+  // resident blocks x partials, then one row of group sums per group
+  const size_t part = ((size_t)sms * (2048 / kMultiThreads) + kMaxGroups) * 2 * kMultiK;
   MB_CUDA_OK(grow_m(&ms.partials, ms.cap_part, part));
   if (!ms.ctl) MB_CUDA_OK(cudaMalloc((void**)&ms.ctl, sizeof(MultiCtl)));
   std::vector<MultiCtl> h(1);
