@@ -614,7 +614,9 @@ __global__ void __launch_bounds__(kThreads)
     float y0[B], y1[B];
     sell_row2<B, U>(A, pt, t, y0, y1);
     const int nr = (2 * t + 1 < A.N) ? 2 : 1;
-    for (int h = 0; h < nr; h++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (h >= nr) break;
 #pragma unroll
       for (int c = 0; c < B; c++) {
         const long long i = (long long)(2 * t + h) * B + c;
@@ -644,7 +646,9 @@ __global__ void __launch_bounds__(kThreads)
     float y0[B], y1[B];
     sell_row2<B, U>(A, stv, q, y0, y1);
     const int nr = (2 * q + 1 < A.N) ? 2 : 1;
-    for (int h = 0; h < nr; h++) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (h >= nr) break;
 #pragma unroll
       for (int c = 0; c < B; c++) {
         const long long i = (long long)(2 * q + h) * B + c;

@@ -104,9 +104,10 @@ __device__ __forceinline__ int2 ld_stream2(const int2* p) { return __ldcs(p); }
 // y0/y1 = (A x) of rows 2t and 2t+1 in FP32 (fused multiply-add). Slots past
 // a row's length hold zero values and a valid column, so both rows run to the
 // longer length.
-template <int B, int U, bool kCoherent = false>
-__device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
-                                          float (&y1)[B]) {
+// The entries of the multiplied vector come from xf(i) (i = column*B + l):
+// a plain gather, or a value computed from other vectors (see sell_row2).
+template <int B, int U, class XF>
+__device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int t, float (&y0)[B], float (&y1)[B]) {
   constexpr int B2 = B * B;
   const int r0 = 2 * t;
   const int lane2 = 2 * (t & 31);
@@ -133,8 +134,8 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
       float x0[B], x1[B];
 #pragma unroll
       for (int l = 0; l < B; l++) {
-        x0[l] = ldx<kCoherent>(x + (long long)j[u].x * B + l);
-        x1[l] = ldx<kCoherent>(x + (long long)j[u].y * B + l);
+        x0[l] = xf((long long)j[u].x * B + l);
+        x1[l] = xf((long long)j[u].y * B + l);
       }
 #pragma unroll
       for (int r = 0; r < B; r++)
@@ -153,8 +154,8 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
     float x0[B], x1[B];
 #pragma unroll
     for (int l = 0; l < B; l++) {
-      x0[l] = ldx<kCoherent>(x + (long long)jj.x * B + l);
-      x1[l] = ldx<kCoherent>(x + (long long)jj.y * B + l);
+      x0[l] = xf((long long)jj.x * B + l);
+      x1[l] = xf((long long)jj.y * B + l);
     }
 #pragma unroll
     for (int r = 0; r < B; r++)
@@ -164,6 +165,12 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
         y1[r] = fmaf(a[r * B + l].y, x1[l], y1[r]);
       }
   }
+}
+
+template <int B, int U, bool kCoherent = false>
+__device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
+                                          float (&y1)[B]) {
+  sell_row2_f<B, U>(A, [&](long long i) { return ldx<kCoherent>(x + i); }, t, y0, y1);
 }
 
 // Block-cooperative staging of the entries of an interleaved vector
