@@ -129,35 +129,18 @@ __device__ __forceinline__ void group_sync(const cg::cluster_group& cl, int gsiz
   else __syncthreads();
 }
 
-// (A64 (x + y))[row] in FP64 with coherent loads of x and y (written by the
-// other CTAs of the cluster during this launch).
-template <int B>
-__device__ __forceinline__ void row_xy64(const SellView<double>& A, const double* x, const float* y, long long row,
-                                         double (&ax)[B]) {
-  constexpr int B2 = B * B;
-  const int lane = (int)(row & (kSlice - 1));
-  const long long base = A.slptr[row >> 5];
-  const int len = A.rowptr[row + 1] - A.rowptr[row];
-#pragma unroll
-  for (int c = 0; c < B; c++) ax[c] = 0.0;
-  for (int k = 0; k < len; k++) {
-    const int j = ld_stream(A.col + base + lane + (long long)k * kSlice);
-    double xs[B];
-#pragma unroll
-    for (int l = 0; l < B; l++)
-      xs[l] = __ldcg(x + (long long)j * B + l) + (double)__ldcg(y + (long long)j * B + l);
-    const double* vk = A.val + (base + (long long)k * kSlice) * B2 + lane;
-#pragma unroll
-    for (int qq = 0; qq < B; qq++)
-#pragma unroll
-      for (int l = 0; l < B; l++) ax[qq] = fma(ld_stream(vk + (qq * B + l) * kSlice), xs[l], ax[qq]);
-  }
-}
+// x + y with coherent loads: both are written by the other CTAs of the
+// cluster during this launch.
+struct XPlusYCoherent {
+  const double* x;
+  const float* y;
+  __device__ __forceinline__ double operator()(long long i) const { return __ldcg(x + i) + (double)__ldcg(y + i); }
+};
 
 // CG on system `si` by a group of gsize CTAs (this one has rank grank).
 template <int B, int U>
-__device__ void solve_system(const BatchArgs& a, int si, int gsize, int grank, const cg::cluster_group& cl,
-                             GroupShared& sh) {
+__device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsize, int grank,
+                                             const cg::cluster_group& cl, GroupShared& sh) {
   const BatchSys S = a.sys[si];
   const long long pair0 = S.row0 / 2, npairs = S.nrows / 2;
   const long long chunk = (npairs + gsize - 1) / gsize;
@@ -179,7 +162,7 @@ __device__ void solve_system(const BatchArgs& a, int si, int gsize, int grank, c
     v[0] = v[1] = 0.0;
     for (long long row = rlo + tid; row < rhi; row += nt) {
       double ax[B];
-      row_xy64<B>(a.A64, a.x, a.y, row, ax);
+      sell_row_f<B, U, double, double>(a.A64, XPlusYCoherent{a.x, a.y}, (int)row, ax);
       float t[B], w[B];
 #pragma unroll
       for (int c = 0; c < B; c++) {
@@ -313,7 +296,7 @@ __device__ void solve_system(const BatchArgs& a, int si, int gsize, int grank, c
 }
 
 template <int B, int U>
-__global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_cg_kernel(const BatchArgs a) {
+__global__ void __launch_bounds__(kBatchMaxThreads, 2) batch_cg_kernel(const BatchArgs a) {
   __shared__ GroupShared sh;
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
@@ -324,11 +307,10 @@ __global__ void __launch_bounds__(kBatchMaxThreads, 1) batch_cg_kernel(const Bat
     cl.sync();  // rank 0 rewrites sh.item only after every CTA has read it
     if (item >= a.nitems) return;
     const BatchItem it = a.items[item];
-    if (!it.split) {
-      solve_system<B, U>(a, a.order[it.first], C, rank, cl, sh);
-    } else if (rank < it.count) {
-      solve_system<B, U>(a, a.order[it.first + rank], 1, 0, cl, sh);
-    }
+    // one call site (inlined): the whole cluster on one system, or one CTA per system
+    const bool mine = !it.split || rank < it.count;
+    if (mine)
+      solve_system<B, U>(a, a.order[it.first + (it.split ? rank : 0)], it.split ? 1 : C, it.split ? 0 : rank, cl, sh);
   }
 }
 

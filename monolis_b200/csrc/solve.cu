@@ -826,9 +826,16 @@ __global__ void __launch_bounds__(kThreads)
 // initial residual (iter == 0) and when the update kernel raised `refresh`;
 // it sits in every iteration on a small grid, so the common case (nothing
 // to do) costs one flag read per block.
+// x + y (FP64 solution plus FP32 correction) as the multiplied vector.
+struct XPlusY {
+  const double* __restrict__ x;
+  const float* __restrict__ y;
+  __device__ __forceinline__ double operator()(long long i) const { return __ldg(x + i) + (double)__ldg(y + i); }
+};
+
 // BiCGSTAB mode (Bicg): the second dot is <r,rt> and the initial refresh
 // also sets the shadow residual rt = r (z unused).
-template <int B, bool Bicg = false>
+template <int B, int U, bool Bicg = false>
 __global__ void __launch_bounds__(kThreads)
     mixed_refresh_kernel(SellView<double> A, const double* __restrict__ x, const float* __restrict__ y,
                          const double* __restrict__ b, float* __restrict__ r, float* __restrict__ z,
@@ -836,27 +843,12 @@ __global__ void __launch_bounds__(kThreads)
                          SolverState* st, double* hist, float* __restrict__ rt = nullptr) {
   if (st->done || !(st->iter == 0 || st->refresh)) return;
   const bool init = st->iter == 0;
-  constexpr int B2 = B * B;
   double v[2] = {0.0, 0.0};
+  const XPlusY xy{x, y};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
-    // (A (x + y))[row] in FP64, blocks in CSR order
-    const int lane = row & (kSlice - 1);
-    const long long base = A.slptr[row >> 5];
-    const int len = A.rowptr[row + 1] - A.rowptr[row];
+    // (A (x + y))[row] in FP64, blocks in CSR order, U slots in flight
     double ax[B];
-#pragma unroll
-    for (int c = 0; c < B; c++) ax[c] = 0.0;
-    for (int k = 0; k < len; k++) {
-      const int j = ld_stream(A.col + base + lane + (long long)k * kSlice);
-      double xs[B];
-#pragma unroll
-      for (int l = 0; l < B; l++) xs[l] = x[(long long)j * B + l] + (double)y[(long long)j * B + l];
-      const double* vk = A.val + (base + (long long)k * kSlice) * B2 + lane;
-#pragma unroll
-      for (int q = 0; q < B; q++)
-#pragma unroll
-        for (int l = 0; l < B; l++) ax[q] = fma(ld_stream(vk + (q * B + l) * kSlice), xs[l], ax[q]);
-    }
+    sell_row_f<B, U, double, double>(A, xy, row, ax);
     float t[B], w[B];
 #pragma unroll
     for (int c = 0; c < B; c++) {
@@ -1085,7 +1077,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_v = mbicg_v_kernel<B, U>;
       auto k_t = mbicg_t_kernel<B, U>;
       auto k_xr = bicg_xr_kernel<B, float, true>;
-      auto k_ref = mixed_refresh_kernel<B, true>;
+      auto k_ref = mixed_refresh_kernel<B, U, true>;
       const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr), g_ref = pgrid(k_ref);
       const int g_p = pgrid(bicg_p_kernel<B, float>), g_s = pgrid(bicg_s_kernel<B, float>);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
@@ -1119,7 +1111,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       const double* b = d_b;
       auto k_spmv = cg_spmv2_kernel<B, U>;
       auto k_upd = mixed_update_kernel<B>;
-      auto k_ref = mixed_refresh_kernel<B>;
+      auto k_ref = mixed_refresh_kernel<B, U>;
       const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
       const int g_ref = pgrid(k_ref);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;

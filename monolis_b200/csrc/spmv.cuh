@@ -40,8 +40,9 @@ inline SellView<double> view_of<double>(const SellMatrix& m) {
 // (src/linalg/matvec.f90:805-823); the FP64 instantiation keeps exactly that
 // sequence of roundings. U slots are loaded before any is consumed so that
 // each thread keeps U*(B*B + 1) independent loads in flight.
-template <int B, int U, class V, class T, bool kCoherent = false>
-__device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restrict__ x, int row, T (&y)[B]) {
+// xf(i) gives entry i = column*B + l of the multiplied vector.
+template <int B, int U, class V, class T, class XF>
+__device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, int row, T (&y)[B]) {
   constexpr int B2 = B * B;
   const int lane = row & (kSlice - 1);
   const long long base = A.slptr[row >> 5];
@@ -64,7 +65,7 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
     for (int u = 0; u < U; u++) {
       T xs[B];
 #pragma unroll
-      for (int l = 0; l < B; l++) xs[l] = ldx<kCoherent>(x + (long long)j[u] * B + l);
+      for (int l = 0; l < B; l++) xs[l] = xf((long long)j[u] * B + l);
 #pragma unroll
       for (int r = 0; r < B; r++)
 #pragma unroll
@@ -78,12 +79,17 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
     for (int e = 0; e < B2; e++) a[e] = ld_stream(v + ((long long)k * B2 + e) * kSlice);
     T xs[B];
 #pragma unroll
-    for (int l = 0; l < B; l++) xs[l] = ldx<kCoherent>(x + (long long)jj * B + l);
+    for (int l = 0; l < B; l++) xs[l] = xf((long long)jj * B + l);
 #pragma unroll
     for (int r = 0; r < B; r++)
 #pragma unroll
       for (int l = 0; l < B; l++) y[r] = add_rn(y[r], mul_rn(T(a[r * B + l]), xs[l]));
   }
+}
+
+template <int B, int U, class V, class T, bool kCoherent = false>
+__device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restrict__ x, int row, T (&y)[B]) {
+  sell_row_f<B, U, V, T>(A, [&](long long i) { return ldx<kCoherent>(x + i); }, row, y);
 }
 
 // Paired FP32 layout (see SellMatrix::d_col2): thread t owns rows 2t and
