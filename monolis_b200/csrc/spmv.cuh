@@ -179,23 +179,6 @@ __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __res
   sell_row2_f<B, U>(A, [&](long long i) { return ldx<kCoherent>(x + i); }, t, y0, y1);
 }
 
-// Block-cooperative staging of the entries of an interleaved vector
-// (x[row*B + c]) that belong to a tile of rows: global memory is read and
-// written as contiguous runs (coalesced), threads then work on whole rows in
-// shared memory. Used for B <= 3; larger blocks access global memory directly.
-template <class T, int B>
-__device__ __forceinline__ void stage_in(T* s, const T* __restrict__ g, long long row0, int nrows) {
-  const long long base = row0 * B;
-  const int len = nrows * B;
-  for (int i = threadIdx.x; i < len; i += blockDim.x) s[i] = g[base + i];
-}
-template <class T, int B>
-__device__ __forceinline__ void stage_out(T* __restrict__ g, const T* s, long long row0, int nrows) {
-  const long long base = row0 * B;
-  const int len = nrows * B;
-  for (int i = threadIdx.x; i < len; i += blockDim.x) g[base + i] = s[i];
-}
-
 // 16-byte vector type of an element type.
 template <class T>
 struct Vec16T;
