@@ -191,6 +191,28 @@ int  monolis_b200_batch_device_solve_R(monolis_b200_batch* batch, double tol, in
 /* device seconds of the last batched solve (CUDA events around the graph launch) */
 double monolis_b200_batch_last_seconds(monolis_b200_batch* batch);
 
+/* ---- device assembly ----
+ * No counterpart in the reference library (its assembly runs on the host).
+ * These work on the library's device copy of the matrix (pattern from the
+ * struct, values kept on the device) and give values bit-identical to the
+ * host calls: monolis_add_matrix_to_sparse_matrix_R element by element in
+ * order, then monolis_set_Dirichlet_bc_R condition by condition in order.
+ * The host mat->mat.R.A is not written (read it back with
+ * monolis_b200_device_get_values); solves and products of this library use
+ * the device values until a host call changes the matrix.
+ *   clear: device values = 0 (the pattern must exist);
+ *   add_elements: d_elem[e*n_base + a] (0-based nodes, device), element e adds
+ *     (d_scale ? d_scale[e] : 1) * d_val[e*val_stride + k] (row-major
+ *     (n_base*ndof)^2, val_stride 0: one shared matrix), all device arrays;
+ *   set_Dirichlet: n_bc conditions (host lists node_id, n_dof_bc, val, in
+ *     call order), d_b the device right-hand side updated in place. */
+int monolis_b200_device_clear_matrix(MONOLIS* mat);
+int monolis_b200_device_add_elements_R(MONOLIS* mat, int n_elem, int n_base, const int* d_elem, const double* d_val,
+                                       long long val_stride, const double* d_scale);
+int monolis_b200_device_set_Dirichlet_bc_R(MONOLIS* mat, double* d_b, int n_bc, const int* node_id,
+                                           const int* n_dof_bc, const double* val);
+int monolis_b200_device_get_values(MONOLIS* mat, double* values);
+
 /* ---- many right-hand sides on one matrix ----
  * No counterpart in the reference library (one right-hand side per solve).
  * Solves A X_k = B_k for k < n_rhs with CG and the struct's preconditioner

@@ -183,6 +183,11 @@ _PRODUCT = {
     "monolis_b200_batch_device_solve_R": (C.c_int, [C.c_void_p, C.c_double, C.c_int, C.c_int, _ip, _dp, _ip]),
     "monolis_b200_batch_last_seconds": (C.c_double, [C.c_void_p]),
     "monolis_b200_solve_multi_R": (C.c_int, [_MP, _CP, C.c_int, _dp, _dp, _ip, _dp, _ip]),
+    "monolis_b200_device_clear_matrix": (C.c_int, [_MP]),
+    "monolis_b200_device_add_elements_R": (C.c_int, [_MP, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_longlong,
+                                                     C.c_void_p]),
+    "monolis_b200_device_set_Dirichlet_bc_R": (C.c_int, [_MP, C.c_void_p, C.c_int, _ip, _ip, _dp]),
+    "monolis_b200_device_get_values": (C.c_int, [_MP, _dp]),
     "monolis_b200_device_solve_multi_R": (C.c_int, [_MP, C.c_int, C.c_void_p, C.c_void_p, _ip, _dp, _ip]),
 }
 

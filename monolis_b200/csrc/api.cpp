@@ -246,6 +246,7 @@ struct DevState {
   mb::SellMatrix AT;  // A^T, built on demand from A's device CSR and the CSC arrays
   long long build_id = 0, at_build_id = -1;
   mb::MultiState* multi = nullptr;  // many-right-hand-side solver buffers
+  bool device_values = false;       // the device values were assembled on the device (not uploaded)
   mb::Scratch sc;
   double* d_b = nullptr;
   double* d_x = nullptr;
@@ -357,13 +358,16 @@ int prepare(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32, double* t_h
       return rc;
     }
   }
-  const bool cached = I[MONOLIS_B200_PRM_I_MATRIX_CACHE] == 1 && s->prepared && s->key_index == a->CSR.index &&
+  // device-assembled values stay until the host changes the matrix
+  const bool keep = I[MONOLIS_B200_PRM_I_MATRIX_CACHE] == 1 || s->device_values;
+  const bool cached = keep && s->prepared && s->key_index == a->CSR.index &&
                       s->key_item == a->CSR.item && s->key_val == a->R.A && s->key_N == a->N &&
                       s->key_ndof == a->NDOF && s->key_version == I[MONOLIS_B200_PRM_I_MATRIX_VERSION];
   cudaStream_t st = ctx().stream;
   if (t_h2d) *t_h2d = 0.0;
   if (!cached) {
     s->prepared = false;
+    s->device_values = false;
     int rc = mb::sell_build(s->A, a->CSR.index, a->CSR.item, a->R.A, a->N, a->NDOF, st, t_h2d);
     if (rc) return rc;
     s->key_index = a->CSR.index;
@@ -1056,6 +1060,67 @@ int monolis_b200_solve_multi_R(MONOLIS* m, MONOLIS_COM* com, int n_rhs, double* 
   cudaFree(d_B);
   cudaFree(d_X);
   return rc;
+}
+
+// ---- device assembly ----
+namespace {
+// Device values changed: rebuild the SELL values (FP32 copy, DIAG factors and
+// the transpose follow on demand).
+int after_device_assembly(MONOLIS* m, DevState* s) {
+  int rc = mb::sell_layout(s->A, ctx().stream);
+  if (rc) return rc;
+  s->device_values = true;
+  s->build_id++;
+  s->key_version = m->prm.Iarray[MONOLIS_B200_PRM_I_MATRIX_VERSION];
+  return MONOLIS_B200_OK;
+}
+}  // namespace
+
+int monolis_b200_device_clear_matrix(MONOLIS* m) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  int rc = prepare(m, s, false, false, nullptr);
+  if (rc) return rc;
+  const size_t nv = (size_t)s->A.nz * m->mat.NDOF * m->mat.NDOF;
+  MB_API_CUDA(cudaMemsetAsync(s->A.d_csrval, 0, nv * sizeof(double), ctx().stream));
+  return after_device_assembly(m, s);
+}
+
+int monolis_b200_device_add_elements_R(MONOLIS* m, int n_elem, int n_base, const int* d_elem, const double* d_val,
+                                       long long val_stride, const double* d_scale) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  int rc = prepare(m, s, false, false, nullptr);
+  if (rc) return rc;
+  rc = mb::device_add_elements(s->A, m->mat.NP, n_elem, n_base, d_elem, d_val, val_stride, d_scale, ctx().stream);
+  if (rc) return rc;
+  return after_device_assembly(m, s);
+}
+
+int monolis_b200_device_set_Dirichlet_bc_R(MONOLIS* m, double* d_b, int n_bc, const int* node_id, const int* n_dof_bc,
+                                           const double* val) {
+  if (n_bc < 0 || (n_bc > 0 && (!node_id || !n_dof_bc || !val))) return MONOLIS_B200_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  int rc = prepare(m, s, false, false, nullptr);
+  if (rc) return rc;
+  rc = mb::device_dirichlet(s->A, d_b, n_bc, node_id, n_dof_bc, val, ctx().stream);
+  if (rc) return rc;
+  return after_device_assembly(m, s);
+}
+
+int monolis_b200_device_get_values(MONOLIS* m, double* values) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared) return MONOLIS_B200_BAD_INPUT;
+  const size_t nv = (size_t)s->A.nz * s->A.ndof * s->A.ndof;
+  MB_API_CUDA(cudaMemcpyAsync(values, s->A.d_csrval, nv * sizeof(double), cudaMemcpyDeviceToHost, ctx().stream));
+  MB_API_CUDA(cudaStreamSynchronize(ctx().stream));
+  return MONOLIS_B200_OK;
 }
 
 int monolis_b200_device_matvec_transpose_R(MONOLIS* m, const double* d_x, double* d_y) {

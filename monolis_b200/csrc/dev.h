@@ -144,6 +144,13 @@ struct SolveResult {
 int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double* d_b, double* d_x,
                  SolveResult& res, double* h_hist, cudaStream_t s);
 
+// ---- device assembly (assemble.cu): values of m's device CSR (d_csrval) ----
+int device_add_elements(SellMatrix& m, int NP, int n_elem, int n_base, const int* d_elem, const double* d_val,
+                        long long val_stride, const double* d_scale, cudaStream_t s);
+// node/dof/val: host lists of n_bc conditions, applied as if in order; d_b device RHS
+int device_dirichlet(SellMatrix& m, double* d_b, int n_bc, const int* node, const int* dof, const double* val,
+                     cudaStream_t s);
+
 // ---- many right-hand sides on one matrix (multi.cu) ----
 struct MultiState;
 MultiState* multi_new();
