@@ -201,6 +201,50 @@ def workload_c3(lib, args, peak):
                         f"rel.res 1e-8, FP64 vs FP32-inner/FP64-refined", "by_peclet": out}
 
 
+def device_assembly_c2(lib, n, b_host):
+    """Elasticity assembled on the device (monolis_b200_device_add_elements_R +
+    monolis_b200_device_set_Dirichlet_bc_R) against the host assembly."""
+    import ctypes as C
+    import torch
+    host = api.Monolis(lib)
+    problems.elasticity(host, n=n)
+    m = api.Monolis(lib)
+    elem = problems.hex_elements(n)
+    m.get_nonzero_pattern_flat(n ** 3, 8, 3, elem)
+    ke = problems.hex8_elasticity_ke(1.0 / (n - 1)).reshape(-1)
+    d_elem = torch.from_numpy(elem).cuda()
+    d_ke = torch.from_numpy(np.ascontiguousarray(ke)).cuda()
+    h = 1.0 / (n - 1)
+    cnt = np.bincount(elem.reshape(-1), minlength=n ** 3).astype(np.float64) * (h ** 3 / 8.0)
+    f = np.zeros((n ** 3, 3))
+    f[:, 2] = -1.0
+    f += problems.normal(2, n ** 3 * 3, 0.0, 0.01).reshape(n ** 3, 3)
+    b0 = np.ascontiguousarray((f * cnt[:, None]).reshape(-1))
+    nodes = np.repeat(np.arange(0, n ** 3, n, dtype=np.int32), 3)
+    dofs = np.tile(np.arange(3, dtype=np.int32), n * n)
+    vals = np.zeros(len(nodes))
+    d_b = torch.from_numpy(b0).cuda()
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = lib.monolis_b200_device_clear_matrix(m.p)
+    rc = rc or lib.monolis_b200_device_add_elements_R(m.p, len(elem), 8, d_elem.data_ptr(), d_ke.data_ptr(), 0, None)
+    rc = rc or lib.monolis_b200_device_set_Dirichlet_bc_R(m.p, d_b.data_ptr(), len(nodes), nodes.ctypes.data_as(ip),
+                                                          dofs.ctypes.data_as(ip), vals.ctypes.data_as(dp))
+    torch.cuda.synchronize()
+    t_dev = time.perf_counter() - t0
+    if rc:
+        return {"failed": int(rc)}
+    vals_dev = np.empty(m.NZ * 9)
+    lib.monolis_b200_device_get_values(m.p, vals_dev.ctypes.data_as(dp))
+    same = bool(np.array_equal(vals_dev.view(np.uint64), host.values().view(np.uint64)) and
+                np.array_equal(d_b.cpu().numpy().view(np.uint64), b_host.view(np.uint64)))
+    m.finalize()
+    host.finalize()
+    return {"device_s": t_dev, "bit_identical_to_host": same,
+            "includes": "clear + 2,048,383 hex8 element matrices (24x24) + 49,152 Dirichlet conditions + layout rebuild"}
+
+
 def fp64_one_by_one(lib, systems, bs, tol):
     """The plain FP64 GPU CG (monolis_b200_device_solve_R) on each system in
     turn, device-resident b and x; returns summed device seconds, iterations."""
@@ -620,6 +664,10 @@ def main():
         spmv[name] = {"seconds": dt, "bytes": byts, "gbs": byts / dt / 1e9}
     peak, peak_kind = measured_peak()
 
+    # device assembly of the same system (element matrices + clamped face),
+    # checked bit for bit against the host-assembled values
+    asm = device_assembly_c2(lib, args.n, b)
+
     # e2e through monolis_solve_R with pinned host buffers (matrix upload included)
     hb = torch.from_numpy(b).pin_memory()
     hx = torch.zeros(n_unk, dtype=torch.float64).pin_memory()
@@ -734,6 +782,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "assembly_s": t_asm,
+            "device_assembly": asm,
             "workloads": workloads,
         }
         print(json.dumps(line), flush=True)
