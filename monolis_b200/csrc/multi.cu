@@ -166,20 +166,6 @@ __device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*t
   return s_ok != 0;
 }
 
-// This block's partial sums (v0, v1 per lane = right-hand side) into partials.
-__device__ __forceinline__ void write_partials(double v0, double v1, double (*s_red)[2][kMultiK], double* partials) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  s_red[w][0][lane] = v0;
-  s_red[w][1][lane] = v1;
-  __syncthreads();
-  if (threadIdx.x < 2 * kMultiK) {
-    const int which = threadIdx.x >> 5, kk = threadIdx.x & 31;
-    double s = 0.0;
-    for (int i = 0; i < nw; i++) s += s_red[i][which][kk];
-    partials[((size_t)blockIdx.x * 2 + which) * kMultiK + kk] = s;
-  }
-}
-
 template <class T>
 __device__ __forceinline__ T fmat(T a, T b, T c);
 template <>
@@ -187,16 +173,45 @@ __device__ __forceinline__ float fmat<float>(float a, float b, float c) { return
 template <>
 __device__ __forceinline__ double fmat<double>(double a, double b, double c) { return fma(a, b, c); }
 
-// Small blocks: at most 64 registers, so that 4 blocks (32 warps) per SM
-// keep enough loads in flight for HBM bandwidth.
-template <int B, class T>
-__global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel(const MultiArgs<T> a) {
+// Four consecutive right-hand sides of one vector entry: one 16-byte access
+// for FP32, two for FP64; kCoherent reads through L2 (values written by other
+// blocks of this launch).
+template <bool kCoherent, class T>
+__device__ __forceinline__ void ld4(const T* p, T (&o)[4]);
+template <bool kCoherent>
+__device__ __forceinline__ void ld4(const float* p, float (&o)[4]) {
+  const float4 v = kCoherent ? __ldcg(reinterpret_cast<const float4*>(p)) : *reinterpret_cast<const float4*>(p);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+template <bool kCoherent>
+__device__ __forceinline__ void ld4(const double* p, double (&o)[4]) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 a = kCoherent ? __ldcg(q) : q[0];
+  const double2 b = kCoherent ? __ldcg(q + 1) : q[1];
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&o)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&o)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(o[0], o[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(o[2], o[3]);
+}
+
+// The kernel. A group of Q lanes owns one block row (a warp works on 32/Q rows
+// at once) and lane q of the group carries right-hand sides 4q..4q+3, so every
+// vector access of a thread is 16 bytes (K is padded to Kp = 4Q; padded
+// right-hand sides are zero and start converged). The row's matrix entries are
+// loaded by the group's lanes, Q at a time, and broadcast with width-Q
+// shuffles; all loops that contain shuffles run to warp-uniform bounds.
+// Small blocks are held to few registers (4 blocks of FP32, 3 of FP64 per
+// SM) so that enough loads are in flight for HBM bandwidth.
+template <int B, class T, int Q>
+__global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 3) : 1)
+    multi_cg_kernel(const MultiArgs<T> a) {
   constexpr int B2 = B * B;
-  constexpr int kCh = B == 1 ? 8 : (B == 2 ? 4 : (B == 3 ? 2 : 1));  // row entries gathered together
-  constexpr int kRows = B == 1 ? 4 : (B <= 3 ? 2 : 1);                // rows per step of the update
-  constexpr int kChR = kCh > 1 ? kCh / 2 : 1;  // the (rare) FP64 refresh: fewer registers
-  // the arrays never alias: tell the compiler, so that loads of the next
-  // rows may move above the stores of the current ones
+  constexpr int Kp = 4 * Q;
+  constexpr int RPW = 32 / Q;  // rows per warp
   const int* __restrict__ rowptr = a.rowptr;
   const int* __restrict__ colv = a.col;
   const T* __restrict__ val = a.val;
@@ -204,108 +219,179 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
   const T* __restrict__ alu = a.alu;
   const double* __restrict__ bv = a.b;
   double* __restrict__ xv = a.x;
-  T* __restrict__ yv_ = a.y;
-  T* __restrict__ rv_ = a.r;
+  T* __restrict__ yv = a.y;
+  T* __restrict__ rv = a.r;
   T* __restrict__ zv = a.z;
-  T* __restrict__ qv_ = a.q;
+  T* __restrict__ qv = a.q;
   __shared__ double s_red[kMultiThreads / 32][2][kMultiK];
   __shared__ double s_tot[2][kMultiK];
   __shared__ int s_flag[2];
-  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const long long W = (long long)gridDim.x * nw;
-  const long long gw = (long long)blockIdx.x * nw + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int qd = lane & (Q - 1);  // quad of right-hand sides
+  const int g = lane / Q;         // row slot within the warp
+  const long long wrow0 = ((long long)blockIdx.x * nw + warp) * RPW;  // first row of this warp
+  const long long sweep = (long long)gridDim.x * nw * RPW;
+  const long long N = a.N;
   const int K = a.K;
-  const bool act = lane < K;
-  const int k = lane;
   MultiCtl* c = a.ctl;
   // the last block of a barrier reads and writes the scalars through a
   // volatile view (L1 is not coherent across SMs); the others use __ldcg
   volatile MultiCtl* vc = c;
-  auto at = [&](long long row, int comp) { return (row * B + comp) * K + k; };
+  auto at = [&](long long row, int comp) { return (row * B + comp) * Kp + 4 * qd; };
+  auto warp_max = [](int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+  };
+  // per-thread sums of its 4 right-hand sides -> partials of the block
+  auto reduce_write = [&](const double (&v0)[4], const double (&v1)[4]) {
+    double w0[4], w1[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      w0[j] = v0[j];
+      w1[j] = v1[j];
+#pragma unroll
+      for (int o = Q; o < 32; o <<= 1) {
+        w0[j] += __shfl_xor_sync(0xffffffffu, w0[j], o);
+        w1[j] += __shfl_xor_sync(0xffffffffu, w1[j], o);
+      }
+    }
+    if (lane < Q)
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        s_red[warp][0][4 * lane + j] = w0[j];
+        s_red[warp][1][4 * lane + j] = w1[j];
+      }
+    __syncthreads();
+    if (threadIdx.x < 2 * kMultiK) {
+      const int which = threadIdx.x >> 5, kk = threadIdx.x & 31;
+      double sum = 0.0;
+      if (kk < Kp)
+        for (int i = 0; i < nw; i++) sum += s_red[i][which][kk];
+      a.partials[((size_t)blockIdx.x * 2 + which) * kMultiK + kk] = sum;
+    }
+  };
+  auto live4 = [&](bool (&lv)[4]) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * qd + j;
+      lv[j] = k < K && __ldcg(&c->done[k]) == 0;
+    }
+  };
 
   // x = y = 0 on the own rows
-  for (long long row = gw; row < a.N; row += W)
-    if (act)
+  for (long long rb = wrow0; rb < N; rb += sweep) {
+    const long long row = rb + g;
+    if (row < N)
 #pragma unroll
       for (int cc = 0; cc < B; cc++) {
-        xv[at(row, cc)] = 0.0;
-        yv_[at(row, cc)] = T(0);
+        const double z4[4] = {0.0, 0.0, 0.0, 0.0};
+        const T t4[4] = {T(0), T(0), T(0), T(0)};
+        st4(xv + at(row, cc), z4);
+        st4(yv + at(row, cc), t4);
       }
+  }
 
-  // r = b - A (x + y) in FP64, z = M^-1 r, for the lanes with `mine` set
-  // (all lanes at the start); partial sums <r,r>, <r,z> written per block
-  auto refresh = [&](bool mine) {
-    double v0 = 0.0, v1 = 0.0;
-    for (long long row = gw; row < a.N; row += W) {
-      const int k0 = rowptr[row], len = rowptr[row + 1] - k0;
-      double ax[B];
+  // r = b - A (x + y) in FP64, z = M^-1 r, for the right-hand sides with
+  // mine[j]; partial sums <r,r>, <r,z> written per block
+  auto refresh = [&](const bool (&mine)[4]) {
+    double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool any = mine[0] || mine[1] || mine[2] || mine[3];
+    for (long long rb = wrow0; rb < N; rb += sweep) {
+      const long long row = rb + g;
+      const bool valid = row < N;
+      const int k0 = valid ? rowptr[row] : 0;
+      const int len = valid ? rowptr[row + 1] - k0 : 0;
+      const int mlen = warp_max(len);
+      double ax[B][4];
 #pragma unroll
-      for (int cc = 0; cc < B; cc++) ax[cc] = 0.0;
-      for (int base = 0; base < len; base += 32) {
-        const int m = min(32, len - base);
-        int cj = 0;
+      for (int cc = 0; cc < B; cc++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) ax[cc][j] = 0.0;
+      for (int base = 0; base < mlen; base += Q) {
+        const bool has = base + qd < len;
+        const int cj = has ? colv[k0 + base + qd] : 0;
         double vv[B2];
 #pragma unroll
-        for (int e = 0; e < B2; e++) vv[e] = 0.0;
-        if (lane < m) {
-          cj = colv[k0 + base + lane];
+        for (int e = 0; e < B2; e++) vv[e] = has ? val64[(long long)(k0 + base + qd) * B2 + e] : 0.0;
 #pragma unroll
-          for (int e = 0; e < B2; e++) vv[e] = val64[(long long)(k0 + base + lane) * B2 + e];
-        }
-        for (int t0 = 0; t0 < m; t0 += kChR) {
-          int jj[kChR];
-          double ae[kChR][B2];
+        for (int u = 0; u < Q; u++) {
+          const int j = __shfl_sync(0xffffffffu, cj, u, Q);
+          double ae[B2];
 #pragma unroll
-          for (int u = 0; u < kChR; u++) {
-            jj[u] = __shfl_sync(0xffffffffu, cj, (t0 + u) & 31);
+          for (int e = 0; e < B2; e++) ae[e] = __shfl_sync(0xffffffffu, vv[e], u, Q);
+          if (base + u < len && any) {
 #pragma unroll
-            for (int e = 0; e < B2; e++) ae[u][e] = __shfl_sync(0xffffffffu, vv[e], (t0 + u) & 31);
-          }
-          if (act && mine) {
-            double xs[kChR][B];
+            for (int l = 0; l < B; l++) {
+              const long long ij = ((long long)j * B + l) * Kp + 4 * qd;
+              double x4[4];
+              T y4[4];
+              ld4<true>(xv + ij, x4);
+              ld4<true>(yv + ij, y4);
 #pragma unroll
-            for (int u = 0; u < kChR; u++)
+              for (int rr = 0; rr < B; rr++)
 #pragma unroll
-              for (int l = 0; l < B; l++) {
-                const long long ij = ((long long)jj[u] * B + l) * K + k;
-                xs[u][l] = __ldcg(xv + ij) + (double)__ldcg(yv_ + ij);
-              }
-#pragma unroll
-            for (int u = 0; u < kChR; u++)
-              if (t0 + u < m)
-#pragma unroll
-                for (int rr = 0; rr < B; rr++)
-#pragma unroll
-                  for (int l = 0; l < B; l++) ax[rr] = fma(ae[u][rr * B + l], xs[u][l], ax[rr]);
+                for (int jj = 0; jj < 4; jj++) ax[rr][jj] = fma(ae[rr * B + l], x4[jj] + (double)y4[jj], ax[rr][jj]);
+            }
           }
         }
       }
-      if (act && mine) {
-        T t[B], w[B];
+      if (valid && any) {
+        double b4[B][4];
+        T t[B][4], w[B][4];
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
-          const double rv = bv[at(row, cc)] - ax[cc];
-          v0 += rv * rv;
-          t[cc] = (T)rv;
-          w[cc] = t[cc];
-          rv_[at(row, cc)] = t[cc];
+          const long long i = at(row, cc);
+          double bb[4];
+          ld4<false>(bv + i, bb);
+          T r4[4], z4[4];
+          ld4<false>(rv + i, r4);
+          ld4<false>(zv + i, z4);
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            b4[cc][j] = bb[j] - ax[cc][j];
+            t[cc][j] = mine[j] ? (T)b4[cc][j] : r4[j];
+            w[cc][j] = mine[j] ? t[cc][j] : z4[j];
+          }
         }
-        if (a.prec) diag_row<B, T>(alu, a.N, (int)row, w);
+        if (a.prec) {
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            if (!mine[j]) continue;
+            T wj[B];
+#pragma unroll
+            for (int cc = 0; cc < B; cc++) wj[cc] = t[cc][j];
+            diag_row<B, T>(alu, a.N, (int)row, wj);
+#pragma unroll
+            for (int cc = 0; cc < B; cc++) w[cc][j] = wj[cc];
+          }
+        }
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
-          zv[at(row, cc)] = w[cc];
-          v1 += (double)t[cc] * (double)w[cc];
+          st4(rv + at(row, cc), t[cc]);
+          st4(zv + at(row, cc), w[cc]);
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (mine[j]) {
+              v0[j] += b4[cc][j] * b4[cc][j];
+              v1[j] += (double)t[cc][j] * (double)w[cc][j];
+            }
         }
       }
     }
-    write_partials(v0, v1, s_red, a.partials);
+    reduce_write(v0, v1);
   };
 
   // the whole grid has zeroed its x and y before any residual reads them
   if (!grid_sync(c, a.partials, false, s_tot, [] {})) return;
-  refresh(true);
+  {
+    bool all[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) all[j] = 4 * qd + j < K;
+    refresh(all);
+  }
   if (!grid_sync(c, a.partials, true, s_tot, [&] {
-        if (threadIdx.x < K) {
+        if (threadIdx.x < kMultiK) {
           const int kk = threadIdx.x;
           const double rr = s_tot[0][kk], rz = s_tot[1][kk];
           vc->B2[kk] = rr;
@@ -314,9 +400,9 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
           vc->fold[kk] = 0;
           vc->refresh[kk] = 0;
           vc->resid[kk] = 0.0;
-          if (!(rr > 0.0) || !isfinite(rr)) {
-            vc->done[kk] = 1;  // B2 == 0: x = 0 solves it
-            vc->status[kk] = isfinite(rr) ? MONOLIS_B200_OK : MONOLIS_B200_NONFINITE;
+          if (kk >= K || !(rr > 0.0) || !isfinite(rr)) {
+            vc->done[kk] = 1;  // B2 == 0: x = 0 solves it (also the padding)
+            vc->status[kk] = (kk >= K || isfinite(rr)) ? MONOLIS_B200_OK : MONOLIS_B200_NONFINITE;
           } else {
             vc->done[kk] = 0;
             vc->status[kk] = MONOLIS_B200_OK;
@@ -331,82 +417,95 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
   T* pold = a.p0;
   T* pnew = a.p1;
   for (;;) {
-    const bool done_k = !act || __ldcg(&c->done[k]) != 0;
+    bool live[4];
+    live4(live);
+    const bool any = live[0] || live[1] || live[2] || live[3];
     const bool first = __ldcg(&c->it) == 1;
-    const T beta = act ? (T)__ldcg(&c->beta[k]) : T(0);
-    const bool fold = act && __ldcg(&c->fold[k]) != 0;
-    // P = Z + beta P (own rows, to pnew); Q = A P with P recomputed from Z
-    // and the old P at the neighbours; <P,Q>
-    double pq = 0.0;
-    for (long long row = gw; row < a.N; row += W) {
-      const int k0 = rowptr[row], len = rowptr[row + 1] - k0;
-      T acc[B];
+    T beta[4];
+    bool fold[4];
 #pragma unroll
-      for (int cc = 0; cc < B; cc++) acc[cc] = T(0);
-      for (int base = 0; base < len; base += 32) {
-        const int m = min(32, len - base);
-        int cj = 0;
+    for (int j = 0; j < 4; j++) {
+      const int k = 4 * qd + j;
+      beta[j] = k < K ? (T)__ldcg(&c->beta[k]) : T(0);
+      fold[j] = k < K && __ldcg(&c->fold[k]) != 0;
+    }
+    // P = Z + beta P (own rows, to pnew); Q = A P with the neighbours' P
+    // recomputed from Z and the old P; <P,Q>
+    double pq[4] = {0.0, 0.0, 0.0, 0.0}, zero4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (long long rb = wrow0; rb < N; rb += sweep) {
+      const long long row = rb + g;
+      const bool valid = row < N;
+      const int k0 = valid ? rowptr[row] : 0;
+      const int len = valid ? rowptr[row + 1] - k0 : 0;
+      const int mlen = warp_max(len);
+      T acc[B][4];
+#pragma unroll
+      for (int cc = 0; cc < B; cc++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[cc][j] = T(0);
+      for (int base = 0; base < mlen; base += Q) {
+        const bool has = base + qd < len;
+        const int cj = has ? colv[k0 + base + qd] : 0;
         T vv[B2];
 #pragma unroll
-        for (int e = 0; e < B2; e++) vv[e] = T(0);
-        if (lane < m) {
-          cj = colv[k0 + base + lane];
+        for (int e = 0; e < B2; e++) vv[e] = has ? val[(long long)(k0 + base + qd) * B2 + e] : T(0);
 #pragma unroll
-          for (int e = 0; e < B2; e++) vv[e] = val[(long long)(k0 + base + lane) * B2 + e];
-        }
-        // kCh entries at a time: all their gathers are issued before any is
-        // used (lanes past the row end hold column 0 and value 0)
-        for (int t0 = 0; t0 < m; t0 += kCh) {
-          int jj[kCh];
-          T ae[kCh][B2];
+        for (int u = 0; u < Q; u++) {
+          const int j = __shfl_sync(0xffffffffu, cj, u, Q);
+          T ae[B2];
 #pragma unroll
-          for (int u = 0; u < kCh; u++) {
-            jj[u] = __shfl_sync(0xffffffffu, cj, (t0 + u) & 31);
+          for (int e = 0; e < B2; e++) ae[e] = __shfl_sync(0xffffffffu, vv[e], u, Q);
+          if (base + u < len && any) {
 #pragma unroll
-            for (int e = 0; e < B2; e++) ae[u][e] = __shfl_sync(0xffffffffu, vv[e], (t0 + u) & 31);
-          }
-          if (!done_k) {
-            T zs[kCh][B], po[kCh][B];
+            for (int l = 0; l < B; l++) {
+              const long long ij = ((long long)j * B + l) * Kp + 4 * qd;
+              T z4[4], p4[4];
+              ld4<true>(zv + ij, z4);
+              if (!first) ld4<true>(pold + ij, p4);
 #pragma unroll
-            for (int u = 0; u < kCh; u++)
+              for (int jj = 0; jj < 4; jj++) {
+                const T pl = first ? z4[jj] : fmat<T>(beta[jj], p4[jj], z4[jj]);
 #pragma unroll
-              for (int l = 0; l < B; l++) {
-                const long long ij = ((long long)jj[u] * B + l) * K + k;
-                zs[u][l] = __ldcg(zv + ij);
-                po[u][l] = first ? T(0) : __ldcg(pold + ij);
-              }
-#pragma unroll
-            for (int u = 0; u < kCh; u++) {
-              if (t0 + u < m) {
-#pragma unroll
-                for (int l = 0; l < B; l++) {
-                  const T pl = first ? zs[u][l] : fmat<T>(beta, po[u][l], zs[u][l]);
-#pragma unroll
-                  for (int rr = 0; rr < B; rr++) acc[rr] = fmat<T>(ae[u][rr * B + l], pl, acc[rr]);
-                }
+                for (int rr = 0; rr < B; rr++) acc[rr][jj] = fmat<T>(ae[rr * B + l], pl, acc[rr][jj]);
               }
             }
           }
         }
       }
-      if (!done_k) {
+      if (valid && any) {
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
           const long long i = at(row, cc);
-          const T pv = first ? zv[i] : fmat<T>(beta, pold[i], zv[i]);
-          pnew[i] = pv;
-          qv_[i] = acc[cc];
-          pq += (double)pv * (double)acc[cc];
-          if (fold) {
-            xv[i] += (double)yv_[i];
-            yv_[i] = T(0);
+          T z4[4], p4[4], pn[4];
+          ld4<false>(zv + i, z4);
+          if (!first) ld4<false>(pold + i, p4);
+#pragma unroll
+          for (int jj = 0; jj < 4; jj++) {
+            pn[jj] = first ? z4[jj] : fmat<T>(beta[jj], p4[jj], z4[jj]);
+            if (live[jj]) pq[jj] += (double)pn[jj] * (double)acc[cc][jj];
+          }
+          st4(pnew + i, pn);
+          st4(qv + i, acc[cc]);
+          if (fold[0] || fold[1] || fold[2] || fold[3]) {
+            double x4[4];
+            T y4[4];
+            ld4<false>(xv + i, x4);
+            ld4<false>(yv + i, y4);
+#pragma unroll
+            for (int jj = 0; jj < 4; jj++)
+              if (fold[jj] && live[jj]) {
+                x4[jj] += (double)y4[jj];
+                y4[jj] = T(0);
+              }
+            st4(xv + i, x4);
+            st4(yv + i, y4);
           }
         }
       }
     }
-    write_partials(pq, 0.0, s_red, a.partials);
+    reduce_write(pq, zero4);
     if (!grid_sync(c, a.partials, true, s_tot, [&] {
-            if (threadIdx.x < K && !vc->done[threadIdx.x]) {
+          if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
             const double w = s_tot[0][kk];
             vc->fold[kk] = 0;
@@ -421,50 +520,62 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
       return;
     // Y += alpha P, R -= alpha Q, Z = M^-1 R; <R,R>, <R,Z>
     {
-      const bool live = act && __ldcg(&c->done[k]) == 0;
-      const T alpha = live ? (T)__ldcg(&c->alpha[k]) : T(0);
-      double v0 = 0.0, v1 = 0.0;
-      // kRows rows per step: the loads of all of them are in flight together
-      for (long long row = gw; live && row < a.N; row += kRows * W) {
-        const int nr = (int)min((long long)kRows, (a.N - row + W - 1) / W);
-        T pv[kRows][B], qv[kRows][B], rv[kRows][B], yv[kRows][B];
+      bool lv[4];
+      live4(lv);
+      const bool anyl = lv[0] || lv[1] || lv[2] || lv[3];
+      T alpha[4];
 #pragma unroll
-        for (int h = 0; h < kRows; h++)
-          if (h < nr)
+      for (int j = 0; j < 4; j++) alpha[j] = lv[j] ? (T)__ldcg(&c->alpha[4 * qd + j]) : T(0);
+      double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+      for (long long rb = wrow0; anyl && rb < N; rb += sweep) {
+        const long long row = rb + g;
+        if (row >= N) continue;
+        T t[B][4], w[B][4];
 #pragma unroll
-            for (int cc = 0; cc < B; cc++) {
-              const long long i = at(row + h * W, cc);
-              pv[h][cc] = pnew[i];
-              qv[h][cc] = qv_[i];
-              rv[h][cc] = rv_[i];
-              yv[h][cc] = yv_[i];
-            }
+        for (int cc = 0; cc < B; cc++) {
+          const long long i = at(row, cc);
+          T p4[4], q4[4], r4[4], y4[4], z4[4];
+          ld4<false>(pnew + i, p4);
+          ld4<false>(qv + i, q4);
+          ld4<false>(rv + i, r4);
+          ld4<false>(yv + i, y4);
+          ld4<false>(zv + i, z4);
 #pragma unroll
-        for (int h = 0; h < kRows; h++) {
-          if (h >= nr) break;
-          const long long rw = row + h * W;
-          T t[B], w[B];
-#pragma unroll
-          for (int cc = 0; cc < B; cc++) {
-            const long long i = at(rw, cc);
-            yv_[i] = fmat<T>(alpha, pv[h][cc], yv[h][cc]);
-            t[cc] = fmat<T>(-alpha, qv[h][cc], rv[h][cc]);
-            rv_[i] = t[cc];
-            w[cc] = t[cc];
+          for (int j = 0; j < 4; j++) {
+            y4[j] = lv[j] ? fmat<T>(alpha[j], p4[j], y4[j]) : y4[j];
+            t[cc][j] = lv[j] ? fmat<T>(-alpha[j], q4[j], r4[j]) : r4[j];
+            w[cc][j] = lv[j] ? t[cc][j] : z4[j];
           }
-          if (a.prec) diag_row<B, T>(alu, a.N, (int)rw, w);
+          st4(yv + i, y4);
+        }
+        if (a.prec) {
 #pragma unroll
-          for (int cc = 0; cc < B; cc++) {
-            zv[at(rw, cc)] = w[cc];
-            v0 += (double)t[cc] * (double)t[cc];
-            v1 += (double)t[cc] * (double)w[cc];
+          for (int j = 0; j < 4; j++) {
+            if (!lv[j]) continue;
+            T wj[B];
+#pragma unroll
+            for (int cc = 0; cc < B; cc++) wj[cc] = t[cc][j];
+            diag_row<B, T>(alu, a.N, (int)row, wj);
+#pragma unroll
+            for (int cc = 0; cc < B; cc++) w[cc][j] = wj[cc];
           }
         }
+#pragma unroll
+        for (int cc = 0; cc < B; cc++) {
+          st4(rv + at(row, cc), t[cc]);
+          st4(zv + at(row, cc), w[cc]);
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (lv[j]) {
+              v0[j] += (double)t[cc][j] * (double)t[cc][j];
+              v1[j] += (double)t[cc][j] * (double)w[cc][j];
+            }
+        }
       }
-      write_partials(v0, v1, s_red, a.partials);
+      reduce_write(v0, v1);
     }
     if (!grid_sync(c, a.partials, true, s_tot, [&] {
-            int any = 0;
+          int any_r = 0;
           if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
             const double rr = s_tot[0][kk], rz = s_tot[1][kk];
@@ -480,7 +591,7 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
               const bool stop = resid < a.tol || it >= a.max_iter;
               if (stop || (a.refine && rn < a.delta * vc->rmax[kk])) {
                 vc->refresh[kk] = 1;  // FP64 residual: convergence test (refine) or the reported residual
-                any = 1;
+                any_r = 1;
               } else {
                 vc->rho1[kk] = vc->rho[kk];
                 vc->rho[kk] = rz;
@@ -488,18 +599,23 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
               }
             }
           }
-          if (threadIdx.x < 32) any = __any_sync(0xffffffffu, any);
+          if (threadIdx.x < 32) any_r = __any_sync(0xffffffffu, any_r);
           if (threadIdx.x == 0) {
-            vc->any_refresh = any;
+            vc->any_refresh = any_r;
             vc->it += 1;
           }
         }))
       return;
     if (__ldcg(&c->any_refresh)) {
-      const bool mine = act && __ldcg(&c->refresh[k]) != 0;
+      bool mine[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k = 4 * qd + j;
+        mine[j] = k < K && __ldcg(&c->refresh[k]) != 0;
+      }
       refresh(mine);
       if (!grid_sync(c, a.partials, true, s_tot, [&] {
-                if (threadIdx.x < K && vc->refresh[threadIdx.x]) {
+            if (threadIdx.x < K && vc->refresh[threadIdx.x]) {
               const int kk = threadIdx.x;
               const double rr = s_tot[0][kk], rz = s_tot[1][kk];
               const double resid = sqrt(rr / vc->B2[kk]);
@@ -541,32 +657,51 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? 4 : 1) multi_cg_kernel
     pnew = tmp;
   }
   // fold the last corrections (every block has passed its last reads of x, y)
-  const bool fold = act && __ldcg(&c->fold[k]) != 0;
-  if (fold)
-    for (long long row = gw; row < a.N; row += W)
+  bool fold[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int k = 4 * qd + j;
+    fold[j] = k < K && __ldcg(&c->fold[k]) != 0;
+  }
+  if (fold[0] || fold[1] || fold[2] || fold[3])
+    for (long long rb = wrow0; rb < N; rb += sweep) {
+      const long long row = rb + g;
+      if (row >= N) continue;
 #pragma unroll
       for (int cc = 0; cc < B; cc++) {
         const long long i = at(row, cc);
-        xv[i] += (double)yv_[i];
-        yv_[i] = T(0);
+        double x4[4];
+        T y4[4];
+        ld4<false>(xv + i, x4);
+        ld4<false>(yv + i, y4);
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+          if (fold[j]) {
+            x4[j] += (double)y4[j];
+            y4[j] = T(0);
+          }
+        st4(xv + i, x4);
+        st4(yv + i, y4);
       }
+    }
 }
 
-// column-major (k slowest) <-> interleaved (k fastest) copies
-__global__ void to_interleaved(const double* __restrict__ src, double* __restrict__ dst, long long n, int K,
+// column-major (k slowest) <-> interleaved (k fastest, stride Kp >= K;
+// the padding right-hand sides are zero)
+__global__ void to_interleaved(const double* __restrict__ src, double* __restrict__ dst, long long n, int K, int Kp,
                                long long ld) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * K; i += (long long)gridDim.x * blockDim.x) {
-    const long long e = i / K;
-    const int k = (int)(i - e * K);
-    dst[i] = src[(long long)k * ld + e];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * Kp; i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i / Kp;
+    const int k = (int)(i - e * Kp);
+    dst[i] = k < K ? src[(long long)k * ld + e] : 0.0;
   }
 }
-__global__ void from_interleaved(const double* __restrict__ src, double* __restrict__ dst, long long n, int K,
+__global__ void from_interleaved(const double* __restrict__ src, double* __restrict__ dst, long long n, int K, int Kp,
                                  long long ld) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * K; i += (long long)gridDim.x * blockDim.x) {
-    const long long e = i / K;
-    const int k = (int)(i - e * K);
-    dst[(long long)k * ld + e] = src[i];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * Kp; i += (long long)gridDim.x * blockDim.x) {
+    const long long e = i / Kp;
+    const int k = (int)(i - e * Kp);
+    if (k < K) dst[(long long)k * ld + e] = src[i];
   }
 }
 __global__ void csr_to_solver(const int* __restrict__ item, const double* __restrict__ val, long long nz, int B2,
@@ -588,9 +723,9 @@ cudaError_t grow_m(P** p, size_t& cap, size_t need) {
   return e;
 }
 
-template <int B, class T>
+template <int B, class T, int Q>
 int launch_multi(const MultiArgs<T>& args, cudaStream_t s) {
-  auto kernel = multi_cg_kernel<B, T>;
+  auto kernel = multi_cg_kernel<B, T, Q>;
   int per_sm = 0, dev = 0, sms = 0;
   MB_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMultiThreads, 0));
   MB_CUDA_OK(cudaGetDevice(&dev));
@@ -656,8 +791,7 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
     MB_CUDA_OK(cudaGetLastError());
     ms.built_for = build_id;
   }
-  const int K = std::min(n_rhs, kMultiK);
-  const size_t nv = (size_t)ld * K;
+  const size_t nv = (size_t)ld * kMultiK;  // capacity for the widest chunk
   const size_t tsize = precision == 1 ? sizeof(float) : sizeof(double);
   MB_CUDA_OK(grow_m(&ms.b, ms.cap_b, nv));
   MB_CUDA_OK(grow_m(&ms.x, ms.cap_x, nv));
@@ -678,7 +812,9 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
   std::vector<MultiCtl> h(1);
   for (int k0 = 0; k0 < n_rhs; k0 += kMultiK) {
     const int Kc = std::min(kMultiK, n_rhs - k0);
-    to_interleaved<<<148 * 8, 256, 0, s>>>(d_B + (long long)k0 * ld, ms.b, ld, Kc, ld);
+    const int Q = Kc <= 8 ? 2 : 8;  // lanes per row; right-hand sides padded to 4Q
+    const int Kp = 4 * Q;
+    to_interleaved<<<148 * 8, 256, 0, s>>>(d_B + (long long)k0 * ld, ms.b, ld, Kc, Kp, ld);
     char* v = static_cast<char*>(ms.vec);
     int rc = dispatch_ndof(nd, [&](auto Bc) -> int {
       constexpr int Bn = decltype(Bc)::value;
@@ -691,7 +827,7 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
         a.y = (float*)(v); a.r = (float*)(v + vec_bytes); a.z = (float*)(v + 2 * vec_bytes);
         a.p0 = (float*)(v + 3 * vec_bytes); a.p1 = (float*)(v + 4 * vec_bytes); a.q = (float*)(v + 5 * vec_bytes);
         a.partials = ms.partials; a.ctl = ms.ctl;
-        return launch_multi<Bn, float>(a, s);
+        return Q == 2 ? launch_multi<Bn, float, 2>(a, s) : launch_multi<Bn, float, 8>(a, s);
       }
       MultiArgs<double> a{};
       a.N = N; a.K = Kc; a.prec = prec; a.refine = 0; a.max_iter = max_iter; a.tol = tol; a.delta = 0.1;
@@ -700,10 +836,10 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
       a.y = (double*)(v); a.r = (double*)(v + vec_bytes); a.z = (double*)(v + 2 * vec_bytes);
       a.p0 = (double*)(v + 3 * vec_bytes); a.p1 = (double*)(v + 4 * vec_bytes); a.q = (double*)(v + 5 * vec_bytes);
       a.partials = ms.partials; a.ctl = ms.ctl;
-      return launch_multi<Bn, double>(a, s);
+      return Q == 2 ? launch_multi<Bn, double, 2>(a, s) : launch_multi<Bn, double, 8>(a, s);
     });
     if (rc) return rc;
-    from_interleaved<<<148 * 8, 256, 0, s>>>(ms.x, d_X + (long long)k0 * ld, ld, Kc, ld);
+    from_interleaved<<<148 * 8, 256, 0, s>>>(ms.x, d_X + (long long)k0 * ld, ld, Kc, Kp, ld);
     MB_CUDA_OK(cudaGetLastError());
     MB_CUDA_OK(cudaMemcpyAsync(h.data(), ms.ctl, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
     MB_CUDA_OK(cudaStreamSynchronize(s));
