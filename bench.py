@@ -274,6 +274,7 @@ def fp64_one_by_one(lib, systems, bs, tol):
 def batch_run(lib, systems, bs, label):
     """Stack the systems into one batch, autotune, solve FP32-refined to 1e-8
     and FP32-only to 1e-6; check every system's FP64 residual in numpy."""
+    import torch
     batch = api.Batch(lib)
     for ix, it, v, _ in systems:
         batch.add_csr(len(ix) - 1, 1, ix, it, v)
@@ -290,7 +291,9 @@ def batch_run(lib, systems, bs, label):
         t_e2e0 = time.perf_counter()
         xs, its, res, st = batch.solve(bs, tol=tol, max_iter=20000, refine=refine)
         t_e2e = time.perf_counter() - t_e2e0
+        torch.cuda.nvtx.range_push(f"c4_batch_{name}")  # ncu --nvtx-include "c4_batch_refined_1e-8/"
         its2, res2, st2 = batch.device_solve(tol=tol, max_iter=20000, refine=refine)
+        torch.cuda.nvtx.range_pop()
         t_dev = batch.last_seconds()
         true = [float(np.linalg.norm(b - problems.csr_matvec(ix, it, v, x)) / np.linalg.norm(b))
                 for (ix, it, v, _), x, b in zip(systems, xs, bs)]
@@ -359,9 +362,11 @@ def multi_rhs_run(lib, sysm, rhs):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+            torch.cuda.nvtx.range_push(f"c4_multi_{name}_{rep}")  # ncu --nvtx-include "c4_multi_refined_1e-8_1/"
             rc = lib.monolis_b200_device_solve_multi_R(m.p, K, d_B.data_ptr(), d_X.data_ptr(),
                                                        its.ctypes.data_as(api._ip), res.ctypes.data_as(api._dp),
                                                        st.ctypes.data_as(api._ip))
+            torch.cuda.nvtx.range_pop()
             e1.record(stream)
             e1.synchronize()
             if rc:
