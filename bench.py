@@ -112,6 +112,17 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
+def max_over_ranks(v, world, device="cuda"):
+    """The slowest rank's value (all ranks take part in the collective)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
 def fixture():
     try:
         with open(FIXTURE) as f:
@@ -691,16 +702,9 @@ def main():
     d2h = n_unk * 8
 
     # max over ranks
-    def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return t.item()
-
-    t_mixed_max = max_over_ranks(t_mixed)
-    t64_max = max_over_ranks(t64)
-    t_e2e_max = max_over_ranks(t_e2e)
+    t_mixed_max = max_over_ranks(t_mixed, world)
+    t64_max = max_over_ranks(t64, world)
+    t_e2e_max = max_over_ranks(t_e2e, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
