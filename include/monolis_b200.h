@@ -227,6 +227,22 @@ int monolis_b200_solve_multi_R(MONOLIS* mat, MONOLIS_COM* com, int n_rhs, double
 int monolis_b200_device_solve_multi_R(MONOLIS* mat, int n_rhs, const double* d_B, double* d_X, int* iter,
                                       double* resid, int* status);
 
+/* ---- multi-rank solve (one process per GPU, NCCL) ----
+ * The reference runs one MPI rank per subdomain, each with the rows it owns
+ * (mat->mat.N) followed by ghost rows (up to mat->mat.NP) and the halo tables
+ * of MONOLIS_COM (recv/send neighbour ranks, offsets and 0-based local node
+ * ids). Attaching an NCCL communicator to a MONOLIS_COM makes
+ * monolis_solve_R(mat, com, b, x) solve the distributed system on the GPUs:
+ * halo updates before every product, dot products summed over the ranks
+ * (FP64 CG; b and x hold NP*ndof entries). Rank 0 creates the id, every rank
+ * receives it (by any means, e.g. MPI or torch.distributed) and calls
+ * monolis_b200_com_init_nccl with its current CUDA device set. NCCL is
+ * loaded at run time (libnccl.so.2). No counterpart in the reference (which
+ * uses MPI). */
+int  monolis_b200_nccl_unique_id(void* id128);
+int  monolis_b200_com_init_nccl(MONOLIS_COM* com, const void* id128, int rank, int size);
+void monolis_b200_com_finalize_nccl(MONOLIS_COM* com);
+
 /* ---- allocation-free inner product ----
  * No counterpart in the reference library.
  * *d_sum = sum_i d_x[i]*d_y[i] for device vectors of length n, enqueued on

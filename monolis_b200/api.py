@@ -188,6 +188,9 @@ _PRODUCT = {
                                                      C.c_void_p]),
     "monolis_b200_device_set_Dirichlet_bc_R": (C.c_int, [_MP, C.c_void_p, C.c_int, _ip, _ip, _dp]),
     "monolis_b200_device_get_values": (C.c_int, [_MP, _dp]),
+    "monolis_b200_nccl_unique_id": (C.c_int, [C.c_void_p]),
+    "monolis_b200_com_init_nccl": (C.c_int, [_CP, C.c_void_p, C.c_int, C.c_int]),
+    "monolis_b200_com_finalize_nccl": (None, [_CP]),
     "monolis_b200_device_solve_multi_R": (C.c_int, [_MP, C.c_int, C.c_void_p, C.c_void_p, _ip, _dp, _ip]),
 }
 
@@ -257,9 +260,43 @@ class Monolis:
 
     def finalize(self):
         if self._alive:
+            if getattr(self, "_halo", None) is not None:
+                if self.lib.is_product:
+                    self.lib.monolis_b200_com_finalize_nccl(C.pointer(self.com))
+                self._restore_com()
             self.lib.monolis_finalize(self.p)
             self.lib.monolis_com_finalize(C.pointer(self.com))
             self._alive = False
+
+    # ---- multi-rank tables (product) ----
+    def set_halo(self, part, rank, size):
+        """Point this struct's MONOLIS_COM at the halo tables of a rank-local
+        system (monolis_b200.partition.partition_rows); the arrays stay owned
+        by Python and are detached again before the struct is finalized."""
+        c = self.com
+        self._halo_saved = (c.recv_index, c.send_index)
+        keep = {k: np.ascontiguousarray(part[k], dtype=np.int32)
+                for k in ("recv_pe", "recv_index", "recv_item", "send_pe", "send_index", "send_item")}
+        self._halo = keep
+        c.my_rank, c.comm_size, c.n_internal_vertex = rank, size, int(part["N"])
+        c.recv_n_neib, c.send_n_neib = len(keep["recv_pe"]), len(keep["send_pe"])
+        c.recv_neib_pe, c.recv_index, c.recv_item = (_iptr(keep["recv_pe"]), _iptr(keep["recv_index"]),
+                                                     _iptr(keep["recv_item"]))
+        c.send_neib_pe, c.send_index, c.send_item = (_iptr(keep["send_pe"]), _iptr(keep["send_index"]),
+                                                     _iptr(keep["send_item"]))
+
+    def _restore_com(self):
+        c = self.com
+        c.recv_index, c.send_index = self._halo_saved
+        c.recv_neib_pe = c.recv_item = c.send_neib_pe = c.send_item = None
+        c.recv_n_neib = c.send_n_neib = 0
+        self._halo = None
+
+    def com_init_nccl(self, uid: bytes, rank, size):
+        buf = C.create_string_buffer(bytes(uid), 128)
+        rc = self.lib.monolis_b200_com_init_nccl(C.pointer(self.com), buf, rank, size)
+        if rc:
+            raise RuntimeError(f"com_init_nccl failed: {STATUS_NAMES.get(rc, rc)}")
 
     def __del__(self):
         try:
@@ -628,6 +665,15 @@ class Batch:
 def _check(rc, what):
     if rc:
         raise RuntimeError(f"{what} failed: {STATUS_NAMES.get(rc, rc)}")
+
+
+def nccl_unique_id(lib: MonolisLib) -> bytes:
+    """An NCCL unique id (128 bytes) for monolis_b200_com_init_nccl."""
+    buf = C.create_string_buffer(128)
+    rc = lib.monolis_b200_nccl_unique_id(buf)
+    if rc:
+        raise RuntimeError(f"nccl_unique_id failed: {STATUS_NAMES.get(rc, rc)}")
+    return buf.raw
 
 
 def stream_handle(lib: MonolisLib) -> int:

@@ -239,6 +239,14 @@ void add_element(MONOLIS_MAT* a, int n1, int n2, const int* e1, const int* e2, c
 }
 
 // ---------------------------------------------------------------------------
+// NCCL communicators attached to MONOLIS_COM tables (multi-rank solve).
+// ---------------------------------------------------------------------------
+std::unordered_map<const MONOLIS_COM*, void*>& nccl_comms() {
+  static std::unordered_map<const MONOLIS_COM*, void*> m;
+  return m;
+}
+
+// ---------------------------------------------------------------------------
 // Device context: one stream, one per-MONOLIS device state.
 // ---------------------------------------------------------------------------
 struct DevState {
@@ -246,6 +254,7 @@ struct DevState {
   mb::SellMatrix AT;  // A^T, built on demand from A's device CSR and the CSC arrays
   long long build_id = 0, at_build_id = -1;
   mb::MultiState* multi = nullptr;  // many-right-hand-side solver buffers
+  mb::ShardPlan shard;              // multi-rank solve: halo buffers and tables
   bool device_values = false;       // the device values were assembled on the device (not uploaded)
   mb::Scratch sc;
   double* d_b = nullptr;
@@ -308,6 +317,7 @@ void state_release(const MONOLIS* m) {
     mb::sell_free(s->A);
     mb::sell_free(s->AT);
     mb::multi_free(s->multi);
+    mb::shard_free(s->shard);
     mb::scratch_free(s->sc);
     cudaFree(s->d_b);
     cudaFree(s->d_x);
@@ -445,7 +455,7 @@ const char* str_prec(int p) {
 // Solve with device b/x already resident; prints and fills prm like
 // src/solver/solver.f90:77-185 + src/define/def_solver_prm.f90:255-355.
 int solve_resident(MONOLIS* m, DevState* s, mb::SellMatrix& A, const double* d_b, double* d_x, double t_start,
-                   double t_prep, double t_h2d) {
+                   double t_prep, double t_h2d, const mb::ShardPlan* shard = nullptr) {
   int* I = m->prm.Iarray;
   double* R = m->prm.Rarray;
   mb::SolveParams p{};
@@ -461,6 +471,8 @@ int solve_resident(MONOLIS* m, DevState* s, mb::SellMatrix& A, const double* d_b
   p.iter_rr = I[MONOLIS_B200_PRM_I_ITER_RR];
   p.timers = I[MONOLIS_B200_PRM_I_KERNEL_TIMERS] == 1;
   p.use_graph = 1;
+  p.shard = shard;
+  p.np_rows = m->mat.NP;
   if (I[MONOLIS_PRM_I_SHOW_SUMMARY] == MONOLIS_I_TRUE)
     printf("** MONOLIS solver: %s, prec: %s\n", str_iter(p.method), str_prec(p.precond));
   const bool log = I[MONOLIS_PRM_I_SHOW_ITERLOG] == MONOLIS_I_TRUE;
@@ -880,8 +892,23 @@ void monolis_inner_product_R(MONOLIS* m, MONOLIS_COM* com, int n_dof, double* x,
 static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool transpose) {
   const double t_start = now_sec();
   int* I = m->prm.Iarray;
-  if (com && com->comm_size > 1) {
-    fprintf(stderr, "** monolis_b200: one rank per solve in this library (comm_size=%d)\n", com->comm_size);
+  // multi-rank: an NCCL communicator attached with monolis_b200_com_init_nccl
+  void* ncomm = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = com ? nccl_comms().find(com) : nccl_comms().end();
+    if (it != nccl_comms().end()) ncomm = it->second;
+  }
+  if (com && com->comm_size > 1 && !ncomm) {
+    fprintf(stderr, "** monolis_b200: comm_size=%d needs an NCCL communicator (monolis_b200_com_init_nccl)\n",
+            com->comm_size);
+    I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
+    return MONOLIS_B200_BAD_INPUT;
+  }
+  const bool sharded = ncomm != nullptr;
+  if (sharded && (transpose || I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_CG ||
+                  I[MONOLIS_B200_PRM_I_PRECISION] != 0)) {
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG\n");
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
     return MONOLIS_B200_BAD_INPUT;
   }
@@ -900,8 +927,20 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   const bool diag = I[MONOLIS_PRM_I_PRECOND] == MONOLIS_PREC_DIAG;
   int rc = prepare(m, s, diag && !transpose, mixed && !transpose, &t_h2d);
   if (!rc && transpose) rc = prepare_transpose(m, s, diag, mixed);
-  const size_t n = (size_t)m->mat.N * m->mat.NDOF;
+  // multi-rank: x and b hold the ghost rows too (NP)
+  const size_t n = (size_t)(sharded ? m->mat.NP : m->mat.N) * m->mat.NDOF;
   if (!rc) rc = ensure_vec(s, n);
+  if (!rc && sharded) {
+    mb::ShardTables t;
+    t.send_pe.assign(com->send_neib_pe, com->send_neib_pe + com->send_n_neib);
+    t.send_ptr.assign(com->send_index, com->send_index + com->send_n_neib + 1);
+    t.send_item.assign(com->send_item, com->send_item + (com->send_n_neib ? com->send_index[com->send_n_neib] : 0));
+    t.recv_pe.assign(com->recv_neib_pe, com->recv_neib_pe + com->recv_n_neib);
+    t.recv_ptr.assign(com->recv_index, com->recv_index + com->recv_n_neib + 1);
+    t.recv_item.assign(com->recv_item, com->recv_item + (com->recv_n_neib ? com->recv_index[com->recv_n_neib] : 0));
+    rc = mb::shard_setup(s->shard, t, m->mat.NDOF);
+    s->shard.comm = ncomm;
+  }
   if (rc) {
     I[MONOLIS_PRM_I_IERR] = rc;
     return rc;
@@ -921,7 +960,8 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   }
   t_h2d += now_sec() - t1;
   const double t_prep = now_sec() - t_start;
-  rc = solve_resident(m, s, transpose ? s->AT : s->A, s->d_b, s->d_x, t_start, t_prep, t_h2d);
+  rc = solve_resident(m, s, transpose ? s->AT : s->A, s->d_b, s->d_x, t_start, t_prep, t_h2d,
+                      sharded ? &s->shard : nullptr);
   if (rc) return rc;
   const double t2 = now_sec();
   cudaMemcpyAsync(x, s->d_x, n * sizeof(double), cudaMemcpyDeviceToHost, st);
@@ -944,6 +984,38 @@ int monolis_b200_solve_transpose_R(MONOLIS* m, MONOLIS_COM* com, double* b, doub
   return solve_host(m, com, b, x, true);
 }
 
+
+// ---- multi-rank communicator ----
+int monolis_b200_nccl_unique_id(void* id128) {
+  if (!id128) return MONOLIS_B200_BAD_INPUT;
+  return mb::shard_unique_id(id128);
+}
+
+int monolis_b200_com_init_nccl(MONOLIS_COM* com, const void* id128, int rank, int size) {
+  if (!com || !id128 || size < 1 || rank < 0 || rank >= size) return MONOLIS_B200_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  void* c = nullptr;
+  int rc = mb::shard_comm_create(&c, id128, rank, size);
+  if (rc) return rc;
+  auto& reg = nccl_comms();
+  auto it = reg.find(com);
+  if (it != reg.end()) mb::shard_comm_destroy(it->second);
+  reg[com] = c;
+  com->my_rank = rank;
+  com->comm_size = size;
+  return MONOLIS_B200_OK;
+}
+
+void monolis_b200_com_finalize_nccl(MONOLIS_COM* com) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  auto& reg = nccl_comms();
+  auto it = reg.find(com);
+  if (it == reg.end()) return;
+  if (ctx().init) cudaStreamSynchronize(ctx().stream);
+  mb::shard_comm_destroy(it->second);
+  reg.erase(it);
+}
 
 // ---- monolis_b200 extensions ----
 int monolis_b200_set_precision(MONOLIS* m, int precision) {

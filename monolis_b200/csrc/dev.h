@@ -46,6 +46,8 @@ struct SolverState {
   int refresh;   // mixed: refresh due in this iteration
   int fold;      // mixed: y still to be folded into x
   int n_refine;  // mixed: refreshes done
+  int sharded;   // multi-rank: reductions leave their local sums in red[] for the all-reduce
+  double red[4];
 };
 
 struct SellMatrix {
@@ -118,6 +120,30 @@ int element_gradient64(int n_elem, int n_base, int ndof, const int* elem, const 
                        cudaStream_t s);
 
 // ---- solvers (device-resident loops) ----
+// ---- row-partitioned (multi-rank) solve (shard.cu) ----
+// Halo tables of one rank: for every neighbour, the local block rows it sends
+// (send_item, 0-based) or receives into (recv_item, ghost rows), with offsets.
+struct ShardTables {
+  std::vector<int> send_pe, send_ptr, send_item, recv_pe, recv_ptr, recv_item;
+};
+struct ShardPlan {
+  void* comm = nullptr;  // ncclComm_t
+  int ndof = 0;
+  std::vector<int> send_pe, recv_pe, send_ptr, recv_ptr;
+  long long n_send = 0, n_recv = 0;
+  int* d_send_item = nullptr;
+  int* d_recv_item = nullptr;
+  void* d_sendbuf = nullptr;
+  void* d_recvbuf = nullptr;
+};
+int shard_unique_id(void* out128);
+int shard_comm_create(void** comm, const void* id128, int rank, int size);
+void shard_comm_destroy(void* comm);
+int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof);
+void shard_free(ShardPlan& sp);
+int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s);
+int shard_allreduce(const ShardPlan& sp, double* d, int k, cudaStream_t s);
+
 struct SolveParams {
   int method;        // MONOLIS_ITER_CG / MONOLIS_ITER_BICGSTAB
   int precond;       // MONOLIS_PREC_NONE / MONOLIS_PREC_DIAG
@@ -131,6 +157,8 @@ struct SolveParams {
   int batch;         // iterations per graph launch
   int use_graph;
   int timers;        // time every kernel with CUDA events (no graph)
+  const ShardPlan* shard = nullptr;  // multi-rank solve (FP64 CG); x holds np_rows block rows (ghosts last)
+  int np_rows = 0;
 };
 struct SolveResult {
   int iter = 0, status = 0, n_refine = 0;

@@ -167,6 +167,11 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // the global sums and the update come after the all-reduce
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
     st->rr_flag = 0;
     if (mode == 0) fin_cg(st, tot[0], tot[1], hist);
     else fin_bicg(st, tot[0], tot[1], hist);
@@ -220,6 +225,10 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {
+      st->red[0] = tot[0];
+      return;
+    }
     st->omega = tot[0];
     st->alpha = st->rho / tot[0];
   });
@@ -313,7 +322,32 @@ __global__ void __launch_bounds__(kThreads)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
     return;
   }
-  grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_cg(st, tot[0], tot[1], hist); });
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
+    fin_cg(st, tot[0], tot[1], hist);
+  });
+}
+
+// Multi-rank CG: the scalar updates, with the sums all-reduced over the ranks
+// (red[] holds them); one thread. Each kernel returns when the phase it
+// follows did not reduce (solve finished, or residual not due).
+__global__ void shard_alpha_kernel(SolverState* st) {
+  if (st->done) return;
+  st->omega = st->red[0];
+  st->alpha = st->rho / st->red[0];
+}
+__global__ void shard_cg_kernel(SolverState* st, double* hist) {
+  if (st->done || (st->iter % st->iter_rr) == 0) return;
+  fin_cg(st, st->red[0], st->red[1], hist);
+}
+__global__ void shard_resid_kernel(SolverState* st, double* hist) {
+  if (st->done || !(st->iter == 0 || st->rr_flag)) return;
+  st->rr_flag = 0;
+  fin_cg(st, st->red[0], st->red[1], hist);
 }
 
 // ---------------------------------------------------------------------------
@@ -962,6 +996,12 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
   if (p.method != 1 && p.method != 5) return kBadInput;
+  if (p.shard && (p.method != 1 || p.precision != 0 || p.np_rows < N)) {
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG\n");
+    return kBadInput;
+  }
+  // vectors gathered by the SpMV hold the ghost rows too
+  const long long n_ext = p.shard ? (long long)p.np_rows * nd : n;
   int rc = scratch_ensure(sc, (size_t)p.max_iter + 2);
   if (rc) return rc;
   if (p.precision == 1) {
@@ -989,9 +1029,10 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   // BiCGSTAB residual norms oscillate: a 0.1 drop below the running maximum
   // comes every few iterations and would refresh needlessly
   h.delta = p.delta > 0 ? p.delta : (p.method == 5 ? 0.01 : 0.1);
+  h.sharded = p.shard ? 1 : 0;
   MB_CUDA_OK(cudaMemcpyAsync(sc.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
   MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * kTicketWords, s));
-  if (p.init_x) MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n, s));
+  if (p.init_x) MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n_ext, s));
 
   Vecs vec{{}, s};
   const int gb = blocks_for(N);
@@ -1014,7 +1055,48 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       const double* b = d_b;
       auto k_resid = resid_kernel<B, U, double, double>;
       const int g_resid = pgrid(k_resid);
-      if (p.method == 1) {
+      if (p.method == 1 && p.shard) {
+        // multi-rank CG: halo updates before the products, all-reduced dots
+        const ShardPlan* sp = p.shard;
+        double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n),
+               *pp = vec.get<double>(n_ext);
+        if (!r || !z || !q || !pp) return kCudaError;
+        if (cudaMemsetAsync(pp, 0, sizeof(double) * n_ext, s) != cudaSuccess) return kCudaError;
+        auto k_spmv = cg_spmv_kernel<B, U, double, double>;
+        auto k_upd = cg_update_kernel<B, double>;
+        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+        int rc2 = shard_halo(*sp, x, s);
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
+        if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+        shard_resid_kernel<<<1, 1, 0, s>>>(st, hist);
+        if (rc2) return rc2;
+        plan.kernels = 5;
+        plan.kind = {1, 0, 2, 1, 0};
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          cg_p_kernel<double><<<gvec, kThreads, 0, ss>>>(n, pp, z, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          shard_halo(*sp, pp, ss);
+          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st);
+          shard_allreduce(*sp, st->red, 1, ss);
+          shard_alpha_kernel<<<1, 1, 0, ss>>>(st);
+          if (ev) cudaEventRecord(ev[2], ss);
+          k_upd<<<g_upd, kThreads, 0, ss>>>(N, x, pp, r, q, z, alu, prec, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[3], ss);
+          if (!special) {
+            shard_allreduce(*sp, st->red, 2, ss);
+            shard_cg_kernel<<<1, 1, 0, ss>>>(st, hist);
+          }
+          if (ev) cudaEventRecord(ev[4], ss);
+          if (special) {
+            shard_halo(*sp, x, ss);
+            k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
+            shard_allreduce(*sp, st->red, 2, ss);
+            shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist);
+          }
+          if (ev) cudaEventRecord(ev[5], ss);
+        };
+      } else if (p.method == 1) {
         double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n), *pp = vec.get<double>(n);
         if (!r || !z || !q || !pp) return kCudaError;
         auto k_spmv = cg_spmv_kernel<B, U, double, double>;

@@ -1,0 +1,158 @@
+"""The multi-rank solve's host-side contract, checked on CPU with gloo ranks:
+monolis_b200.partition builds rank-local systems and MONOLIS_COM halo tables
+whose halo exchange (pack send_item -> neighbour -> unpack into recv_item)
+and per-rank dot products, followed by the scalar updates the device code
+applies (FP64 CG with block-Jacobi), reproduce the single-rank solve of the
+oracle: same solution to 1e-10, iteration count within 2."""
+import os
+import sys
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "_build", "libmonolis_oracle.so")
+
+
+def global_system(problem):
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from monolis_b200 import api
+    from monolis_b200 import problems as P
+    lib = api.load_library(ORACLE, oracle=True)
+    m = api.Monolis(lib)
+    b = P.laplacian(m, n=7) if problem == "laplacian" else P.elasticity(m, n=5)
+    return m, np.ascontiguousarray(b)
+
+
+def local_matvec(p, nd, x):
+    """y (owned rows) = A_local x (owned + ghost entries)."""
+    n, ix, it, v = p["N"], p["index"], p["item"], p["val"].reshape(-1, nd, nd)
+    y = np.zeros((n, nd))
+    xb = x.reshape(-1, nd)
+    for i in range(n):
+        for k in range(ix[i], ix[i + 1]):
+            y[i] += v[k] @ xb[it[k]]
+    return y.reshape(-1)
+
+
+def _worker(rank, world, port, problem, q):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        if ROOT not in sys.path:
+            sys.path.insert(0, ROOT)
+        from monolis_b200 import partition
+        m, b = global_system(problem)
+        nd = m.NDOF
+        parts = partition.partition_rows(m.csr_index(), m.csr_item() - 1, m.values(), nd, world)
+        p = parts[rank]
+        n, npr = p["N"], p["NP"]
+        bl = np.zeros(npr * nd)
+        bl[:n * nd] = b[p["glob"][:n].repeat(nd) * nd + np.tile(np.arange(nd), n)]
+
+        def halo(v):
+            reqs, bufs = [], []
+            for qd, s in enumerate(p["send_pe"]):
+                items = p["send_item"][p["send_index"][qd]:p["send_index"][qd + 1]]
+                buf = torch.from_numpy(np.ascontiguousarray(v.reshape(-1, nd)[items].reshape(-1)))
+                reqs.append(dist.isend(buf, int(s)))
+                bufs.append(buf)
+            for qd, s in enumerate(p["recv_pe"]):
+                items = p["recv_item"][p["recv_index"][qd]:p["recv_index"][qd + 1]]
+                buf = torch.empty(len(items) * nd, dtype=torch.float64)
+                dist.recv(buf, int(s))
+                v.reshape(-1, nd)[items] = buf.numpy().reshape(-1, nd)
+            for r_ in reqs:
+                r_.wait()
+
+        def gdot(a, c):
+            t = torch.tensor([float(np.dot(a[:n * nd], c[:n * nd]))], dtype=torch.float64)
+            dist.all_reduce(t)
+            return t.item()
+
+        # block-Jacobi factors of the owned diagonal blocks (inverse blocks)
+        vb = p["val"].reshape(-1, nd, nd)
+        dinv = np.zeros((n, nd, nd))
+        for i in range(n):
+            for k in range(p["index"][i], p["index"][i + 1]):
+                if p["item"][k] == i:
+                    dinv[i] = np.linalg.inv(vb[k])
+        prec = lambda r_: np.einsum("iab,ib->ia", dinv, r_[:n * nd].reshape(n, nd)).reshape(-1)
+        x = np.zeros(npr * nd)
+        halo(x)
+        r = bl[:n * nd] - local_matvec(p, nd, x)
+        z = prec(r)
+        B2 = gdot(bl, bl)
+        rho = gdot(r, z)
+        pvec = np.zeros(npr * nd)
+        it = 0
+        while it < 5000:
+            it += 1
+            pvec[:n * nd] = z if it == 1 else z + (rho / rho_old) * pvec[:n * nd]
+            halo(pvec)
+            qv = local_matvec(p, nd, pvec)
+            alpha = rho / gdot(pvec, qv)
+            x[:n * nd] += alpha * pvec[:n * nd]
+            r -= alpha * qv
+            z = prec(r)
+            rr = gdot(r, r)
+            rho_old, rho = rho, gdot(r, z)
+            if np.sqrt(rr / B2) < 1e-8:
+                break
+        q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("problem,world", [("laplacian", 2), ("laplacian", 3), ("elasticity", 2)])
+def test_partitioned_cg_matches_single_rank(problem, world, oracle):
+    from monolis_b200 import api
+    from helpers import solve
+    m, b = global_system(problem)
+    nd = m.NDOF
+    x_ref, it_ref, _, st = solve(m, b, api.ITER_CG, api.PREC_DIAG, tol=1e-8)
+    assert st == 0
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30500 + (os.getpid() % 2000) + 7 * world
+    procs = [ctx.Process(target=_worker, args=(r, world, port, problem, q)) for r in range(world)]
+    for p_ in procs:
+        p_.start()
+    out = [q.get(timeout=180) for _ in range(world)]
+    for p_ in procs:
+        p_.join(timeout=60)
+        assert p_.exitcode == 0
+    x = np.zeros_like(b)
+    its = set()
+    for rank, glob, xl, it in out:
+        glob = np.array(glob)
+        x[(glob[:, None] * nd + np.arange(nd)).reshape(-1)] = xl
+        its.add(it)
+    assert len(its) == 1  # every rank stops at the same iteration
+    assert abs(its.pop() - it_ref) <= 2
+    x_tight, _, _, _ = solve(m, b, api.ITER_CG, api.PREC_DIAG, tol=1e-12)
+    assert np.linalg.norm(x - x_tight) / np.linalg.norm(x_tight) < 1e-6
+
+
+def test_partition_tables_are_consistent():
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from monolis_b200 import partition
+    m, b = global_system("laplacian")
+    parts = partition.partition_rows(m.csr_index(), m.csr_item() - 1, m.values(), 1, 4)
+    assert sum(p["N"] for p in parts) == m.N
+    for r, p in enumerate(parts):
+        # what r receives from s is exactly what s sends to r, in the same order
+        for qd, s in enumerate(p["recv_pe"]):
+            recv_glob = p["glob"][p["recv_item"][p["recv_index"][qd]:p["recv_index"][qd + 1]]]
+            ps = parts[s]
+            k = list(ps["send_pe"]).index(r)
+            send_glob = ps["glob"][ps["send_item"][ps["send_index"][k]:ps["send_index"][k + 1]]]
+            assert np.array_equal(recv_glob, send_glob)
+        assert np.all(p["item"] < p["NP"])
