@@ -399,7 +399,7 @@ int dispatch_batch(int ndof, int u, F&& f) {
   return dispatch_ndof(ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
     return dispatch_u(u, [&](auto Uc) {
-      constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
+      constexpr int U = eff_u(B, decltype(Uc)::value);
       return f(batch_cg_kernel<B, U>);
     });
   });

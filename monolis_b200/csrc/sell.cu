@@ -146,28 +146,41 @@ __global__ void diag_setup_kernel(const int* __restrict__ rowptr, const int* __r
   for (int e = 0; e < B2; e++) alu[(long long)e * N + i] = LU[e];
 }
 
+// Grid-stride loops: launched with one thread per row (pair) for a plain
+// product, or with a persistent grid when the unroll depth is tuned for the
+// solver kernels, which all run persistent grids.
 template <int B, int U, class V, class T>
 __global__ void __launch_bounds__(256) spmv_kernel(SellView<V> A, const T* __restrict__ x, T* __restrict__ y) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= A.N) return;
-  T acc[B];
-  sell_row<B, U, V, T>(A, x, row, acc);
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+    T acc[B];
+    sell_row<B, U, V, T>(A, x, row, acc);
 #pragma unroll
-  for (int r = 0; r < B; r++) y[(long long)row * B + r] = acc[r];
+    for (int r = 0; r < B; r++) y[(long long)row * B + r] = acc[r];
+  }
 }
 
 template <int B, int U>
 __global__ void __launch_bounds__(256) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (2 * t >= A.N) return;
-  float y0[B], y1[B];
-  sell_row2<B, U>(A, x, t, y0, y1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; 2 * t < A.N; t += gridDim.x * blockDim.x) {
+    float y0[B], y1[B];
+    sell_row2<B, U>(A, x, t, y0, y1);
 #pragma unroll
-  for (int r = 0; r < B; r++) y[(long long)2 * t * B + r] = y0[r];
-  if (2 * t + 1 < A.N) {
+    for (int r = 0; r < B; r++) y[(long long)2 * t * B + r] = y0[r];
+    if (2 * t + 1 < A.N) {
 #pragma unroll
-    for (int r = 0; r < B; r++) y[(long long)(2 * t + 1) * B + r] = y1[r];
+      for (int r = 0; r < B; r++) y[(long long)(2 * t + 1) * B + r] = y1[r];
+    }
   }
+}
+
+// Resident blocks of 256 threads per SM x SMs.
+template <class K>
+int persistent_blocks(K kernel) {
+  int b = 0, d = 0, sms = 0;
+  cudaGetDevice(&d);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess || b < 1) b = 1;
+  return b * (sms > 0 ? sms : 148);
 }
 
 template <class T>
@@ -334,13 +347,14 @@ void sell_free(SellMatrix& m) {
 }
 
 
-int spmv64_u(const SellMatrix& m, int u, const double* x, double* y, cudaStream_t s) {
+int spmv64_u(const SellMatrix& m, int u, const double* x, double* y, cudaStream_t s, bool persistent = false) {
   SellView<double> A = view_of<double>(m);
   int rc = dispatch_ndof(m.ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
     return dispatch_u(u, [&](auto Uc) {
-      constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
-      spmv_kernel<B, U, double, double><<<(m.N + 255) / 256, 256, 0, s>>>(A, x, y);
+      constexpr int U = eff_u(B, decltype(Uc)::value);
+      auto k = spmv_kernel<B, U, double, double>;
+      k<<<persistent ? persistent_blocks(k) : (m.N + 255) / 256, 256, 0, s>>>(A, x, y);
       return (int)kOk;
     });
   });
@@ -349,15 +363,16 @@ int spmv64_u(const SellMatrix& m, int u, const double* x, double* y, cudaStream_
   return kOk;
 }
 
-int spmv32_u(const SellMatrix& m, int u, const float* x, float* y, cudaStream_t s) {
+int spmv32_u(const SellMatrix& m, int u, const float* x, float* y, cudaStream_t s, bool persistent = false) {
   if (!m.have_val32) return kBadInput;
   SellView2 A = view2_of(m);
   const int threads = (m.N + 1) / 2;
   int rc = dispatch_ndof(m.ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
     return dispatch_u(u, [&](auto Uc) {
-      constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
-      spmv2_kernel<B, U><<<(threads + 255) / 256, 256, 0, s>>>(A, x, y);
+      constexpr int U = eff_u(B, decltype(Uc)::value);
+      auto k = spmv2_kernel<B, U>;
+      k<<<persistent ? persistent_blocks(k) : (threads + 255) / 256, 256, 0, s>>>(A, x, y);
       return (int)kOk;
     });
   });
@@ -369,8 +384,11 @@ int spmv32_u(const SellMatrix& m, int u, const float* x, float* y, cudaStream_t 
 int spmv64(const SellMatrix& m, const double* x, double* y, cudaStream_t s) { return spmv64_u(m, m.u64, x, y, s); }
 int spmv32(const SellMatrix& m, const float* x, float* y, cudaStream_t s) { return spmv32_u(m, m.u32, x, y, s); }
 
-// Unroll depth per matrix: each variant is launched 3 times on zero vectors
-// (the kernels have no data-dependent control flow) and the fastest kept.
+// Unroll depth per matrix (1, 2, 3 slots in flight; also 4 and 8 for 1x1
+// blocks): each variant is launched 3 times on zero vectors (the kernels have
+// no data-dependent control flow) and the fastest kept. The launches use the
+// persistent grid of the solver kernels: a one-thread-per-row grid streams
+// the matrix at the HBM rate for every depth and would not tell them apart.
 int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s) {
   if (m.ndof >= 4) {
     m.u64 = m.u32 = 1;
@@ -388,9 +406,14 @@ int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s) {
   float best = 1e30f;
   int best_u = 2;
   int rc = kOk;
-  for (int u = 1; u <= 3 && rc == kOk; u++) {
+  static const int cand1[] = {1, 2, 3, 4, 8}, cand23[] = {1, 2, 3};
+  const int* cand = m.ndof == 1 ? cand1 : cand23;
+  const int ncand = m.ndof == 1 ? 5 : 3;
+  for (int ci = 0; ci < ncand && rc == kOk; ci++) {
+    const int u = cand[ci];
     auto run = [&]() {
-      return fp32 ? spmv32_u(m, u, (const float*)x, (float*)y, s) : spmv64_u(m, u, (const double*)x, (double*)y, s);
+      return fp32 ? spmv32_u(m, u, (const float*)x, (float*)y, s, true)
+                  : spmv64_u(m, u, (const double*)x, (double*)y, s, true);
     };
     rc = run();  // warm
     if (rc) break;

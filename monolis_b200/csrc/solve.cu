@@ -1042,7 +1042,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   rc = dispatch_ndof(nd, [&](auto Bc) -> int {
    constexpr int B = decltype(Bc)::value;
    return dispatch_u(p.precision == 0 ? m.u64 : m.u32, [&](auto Uc) -> int {
-    constexpr int U = B >= 4 ? 1 : decltype(Uc)::value;
+    constexpr int U = eff_u(B, decltype(Uc)::value);
     SellView<double> A64 = view_of<double>(m);
     double* partials = sc.partials;
     unsigned int* ticket = sc.ticket;

@@ -72,18 +72,31 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
         for (int l = 0; l < B; l++) y[r] = add_rn(y[r], mul_rn(T(a[u][r * B + l]), xs[l]));
     }
   }
-  for (; k < len; k++) {
-    const int jj = ld_stream(c + (long long)k * kSlice);
-    V a[B2];
+  // the last, partial chunk: its loads are issued together (predicated; slots
+  // past the row end are not read) and only the row's slots are added, in order
+  const int rem = len - k;
+  if (U > 1 && rem > 0) {
+    int j[U];
+    V a[U][B2];
 #pragma unroll
-    for (int e = 0; e < B2; e++) a[e] = ld_stream(v + ((long long)k * B2 + e) * kSlice);
-    T xs[B];
+    for (int u = 0; u < U; u++) {
+      j[u] = u < rem ? ld_stream(c + (long long)(k + u) * kSlice) : 0;
 #pragma unroll
-    for (int l = 0; l < B; l++) xs[l] = xf((long long)jj * B + l);
+      for (int e = 0; e < B2; e++) a[u][e] = u < rem ? ld_stream(v + ((long long)(k + u) * B2 + e) * kSlice) : V(0);
+    }
+    T xs[U][B];
 #pragma unroll
-    for (int r = 0; r < B; r++)
+    for (int u = 0; u < U; u++)
 #pragma unroll
-      for (int l = 0; l < B; l++) y[r] = add_rn(y[r], mul_rn(T(a[r * B + l]), xs[l]));
+      for (int l = 0; l < B; l++) xs[u][l] = u < rem ? xf((long long)j[u] * B + l) : T(0);
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (u >= rem) break;
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int l = 0; l < B; l++) y[r] = add_rn(y[r], mul_rn(T(a[u][r * B + l]), xs[u][l]));
+    }
   }
 }
 
@@ -152,24 +165,37 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
         }
     }
   }
-  for (; k < len; k++) {
-    const int2 jj = ld_stream2(c + (long long)k * 32);
-    float2 a[B2];
+  // the last, partial chunk: loads issued together, slots past the end not read
+  const int rem = len - k;
+  if (rem > 0) {
+    int2 j[U];
+    float2 a[U][B2];
 #pragma unroll
-    for (int e = 0; e < B2; e++) a[e] = ld_stream2(v + ((long long)k * B2 + e) * 32);
-    float x0[B], x1[B];
+    for (int u = 0; u < U; u++) {
+      j[u] = u < rem ? ld_stream2(c + (long long)(k + u) * 32) : make_int2(0, 0);
 #pragma unroll
-    for (int l = 0; l < B; l++) {
-      x0[l] = xf((long long)jj.x * B + l);
-      x1[l] = xf((long long)jj.y * B + l);
+      for (int e = 0; e < B2; e++)
+        a[u][e] = u < rem ? ld_stream2(v + ((long long)(k + u) * B2 + e) * 32) : make_float2(0.f, 0.f);
     }
+    float x0[U][B], x1[U][B];
 #pragma unroll
-    for (int r = 0; r < B; r++)
+    for (int u = 0; u < U; u++)
 #pragma unroll
       for (int l = 0; l < B; l++) {
-        y0[r] = fmaf(a[r * B + l].x, x0[l], y0[r]);
-        y1[r] = fmaf(a[r * B + l].y, x1[l], y1[r]);
+        x0[u][l] = u < rem ? xf((long long)j[u].x * B + l) : 0.f;
+        x1[u][l] = u < rem ? xf((long long)j[u].y * B + l) : 0.f;
       }
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (u >= rem) break;
+#pragma unroll
+      for (int r = 0; r < B; r++)
+#pragma unroll
+        for (int l = 0; l < B; l++) {
+          y0[r] = fmaf(a[u][r * B + l].x, x0[u][l], y0[r]);
+          y1[r] = fmaf(a[u][r * B + l].y, x1[u][l], y1[r]);
+        }
+    }
   }
 }
 
@@ -300,8 +326,15 @@ inline int dispatch_u(int u, F&& f) {
   switch (u) {
     case 1: return f(std::integral_constant<int, 1>{});
     case 3: return f(std::integral_constant<int, 3>{});
+    case 4: return f(std::integral_constant<int, 4>{});
+    case 8: return f(std::integral_constant<int, 8>{});
     default: return f(std::integral_constant<int, 2>{});
   }
 }
+
+// Unroll depth actually used for block size B: deep unrolls (4, 8 slots in
+// flight) only for 1x1 blocks, where a row has few slots and registers are
+// plentiful; 2x2 and 3x3 blocks stop at 3, larger blocks at 1.
+constexpr int eff_u(int B, int u) { return B >= 4 ? 1 : (B >= 2 && u > 3 ? 3 : u); }
 
 }  // namespace mb
