@@ -38,9 +38,9 @@ FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")
 METRIC = "time to rel.res 1e-8, FP32-refined block-CSR CG (3D elasticity 128^3 nodes, ndof=3)"
 TOL = 1e-8
 # DRAM bytes (read + write) per launch of cg_spmv2_kernel divided by its
-# algorithmic bytes, from the ncu --set full capture at 64^3 nodes
-# (287.25 MB / 281.74 MB); traffic scales with the blocks processed.
-NCU_SPMV2_TRAFFIC_RATIO = 1.0195
+# layout bytes, from the ncu --set full capture at 64^3 nodes
+# (271.92 MB / 268.45 MB); traffic scales with the blocks processed.
+NCU_SPMV2_TRAFFIC_RATIO = 1.0129
 
 
 def log(*a):
@@ -199,7 +199,9 @@ def workload_c3(lib, args, peak):
                 kt, _ = kernel_times(m, stream, d_b, d_x)
                 res[name]["kernel_us_per_iteration"] = {"p": kt[0] * 1e6, "v=A*pt": kt[1] * 1e6, "s": kt[2] * 1e6,
                                                         "t=A*st": kt[3] * 1e6, "x,r": kt[4] * 1e6}
-                byts = problems.spmv_bytes(m.NZ, m.N, 1, 8)
+                byts = float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64])
+                res[name]["spmv_layout_bytes"] = byts
+                res[name]["wide_slices"] = int(m.Iarray[api.B200_PRM_I_WIDE_SLICES_FP64])
                 res[name]["spmv_in_solve_gbs"] = byts / kt[1] / 1e9
                 res[name]["spmv_in_solve_frac_of_measured"] = byts / kt[1] / 1e9 / peak
         res["mixed"]["rel_error_vs_fp64_solution"] = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
@@ -658,6 +660,15 @@ def main():
     # SpMV roofline (standalone kernels, FP64 and FP32), CUDA events on the library stream
     nzb, padded, nslices = m.device_info()
     u64, u32 = int(m.Iarray[api.B200_PRM_I_UNROLL_FP64]), int(m.Iarray[api.B200_PRM_I_UNROLL_FP32])
+    # HBM bytes of one SpMV in the device layouts (16-bit column differences
+    # where a slice allows them), reported by the library after prepare
+    layout_bytes = {"fp64": float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64]),
+                    "fp32": float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP32])}
+    layout = {"bytes_fp64": layout_bytes["fp64"], "bytes_fp32": layout_bytes["fp32"],
+              "bytes_fp64_32bit_columns": problems.spmv_bytes(nz, N, nd, 8),
+              "bytes_fp32_32bit_columns": problems.spmv_bytes(nz, N, nd, 4),
+              "wide_slices_fp64": int(m.Iarray[api.B200_PRM_I_WIDE_SLICES_FP64]),
+              "wide_slices_fp32": int(m.Iarray[api.B200_PRM_I_WIDE_SLICES_FP32])}
     xs64 = torch.randn(n_unk, dtype=torch.float64, device="cuda")
     ys64 = torch.empty_like(xs64)
     xs32 = xs64.float()
@@ -676,7 +687,7 @@ def main():
         e1.record(stream)
         e1.synchronize()
         dt = e0.elapsed_time(e1) * 1e-3 / reps
-        byts = problems.spmv_bytes(nz, N, nd, vb)
+        byts = layout_bytes[name]
         spmv[name] = {"seconds": dt, "bytes": byts, "gbs": byts / dt / 1e9}
     peak, peak_kind = measured_peak()
 
@@ -748,8 +759,8 @@ def main():
             log(f"[rank 0] workload {w}: {json.dumps(workloads[w])[:400]}")
 
     if rank == 0:
-        spmv32_bytes = problems.spmv_bytes(nz, N, nd, 4)
-        spmv64_bytes = problems.spmv_bytes(nz, N, nd, 8)
+        spmv32_bytes = layout_bytes["fp32"]
+        spmv64_bytes = layout_bytes["fp64"]
         in_solve = {
             "mixed_us_per_iteration": {"p+fold": kt32[0] * 1e6, "q=A*p (fp32, +<p,q>)": kt32[1] * 1e6,
                                        "update (+M^-1, dots)": kt32[2] * 1e6, "refresh (gated)": kt32[3] * 1e6},
@@ -766,7 +777,7 @@ def main():
                                    f"{nz} 3x3 blocks, CG + 3x3 block-Jacobi, rel.res 1e-8",
                        "unknowns": n_unk, "nz_blocks": nz, "padded_blocks": padded,
                        "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (matrix 4.3 GB FP64 + 2.3 GB FP32)"},
+                       "l2": "inputs larger than L2 (matrix 4.2 GB FP64 + 2.2 GB FP32)"},
             "iterations": int(np.median(iters)), "fp64_refreshes": nref, "true_rel_residual": true_res,
             "rel_error_vs_fp64_solution": err_vs_fp64,
             "fp64": {"value": t64_max, "unit": "s", "iterations": it64, "rel_residual": res64},
@@ -778,12 +789,13 @@ def main():
                          "unit": "GB/s", "frac": in_solve["spmv_fp32_in_solve_gbs"] / peak,
                          "traffic": NCU_SPMV2_TRAFFIC_RATIO * spmv32_bytes,
                          "traffic_source": "ncu --set full capture of cg_spmv2_kernel at 64^3 nodes "
-                                           "(dram read+write / algorithmic bytes = 1.019), scaled by the "
-                                           "algorithmic bytes of a 128^3 launch",
+                                           "(dram read+write / layout bytes = 1.013), scaled by the "
+                                           "layout bytes of a 128^3 launch",
                          "kernel": "cg_spmv2_kernel (FP32 paired sliced-ELL SpMV q=A*p with fused <p,q>), "
                                    "average launch inside a mixed solve, kernel-timer mode",
                          "algorithmic_bytes_per_launch": spmv32_bytes, "peak_kind": peak_kind},
             "in_solve_kernels": in_solve,
+            "spmv_layout": layout,
             "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call"},
             "gpu_launches": launches,

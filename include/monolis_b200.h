@@ -40,6 +40,9 @@ static const int MONOLIS_B200_PRM_I_KERNEL_TIMERS  = 40; /* 1: time every kernel
                                                             fills TIME_SPMV / DOTP / PREC and TIME_KERNEL+k */
 static const int MONOLIS_B200_PRM_I_REFRESH_PERIOD = 41; /* mixed precision: FP64 residual refresh at the latest
                                                             n iterations after the previous one (0: no limit) */
+static const int MONOLIS_B200_PRM_I_WIDE_SLICES_FP64 = 42; /* out: 32-row slices that keep 32-bit column ids (the
+                                                              others store 16-bit differences to a base per slot) */
+static const int MONOLIS_B200_PRM_I_WIDE_SLICES_FP32 = 43; /* out: same for the 64-row slices of the FP32 layout */
 
 static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
                                                             below delta * its largest value since the last one
@@ -47,6 +50,9 @@ static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP6
 static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */
 static const int MONOLIS_B200_PRM_R_TIME_D2H       = 32; /* out: seconds spent on device->host copies */
 static const int MONOLIS_B200_PRM_R_TIME_LOOP      = 33; /* out: seconds in the device iteration loop */
+static const int MONOLIS_B200_PRM_R_SPMV_BYTES_FP64 = 34; /* out: HBM bytes of one FP64 SpMV in the device layout:
+                                                              values, column ids, row and slice offsets, x, y */
+static const int MONOLIS_B200_PRM_R_SPMV_BYTES_FP32 = 35; /* out: same for the FP32 layout (0 before it is built) */
 static const int MONOLIS_B200_PRM_R_TIME_KERNEL    = 40; /* out, timing mode: seconds per kernel slot k of an
                                                             iteration in Rarray[40 + k], k < 8 */
 

@@ -50,10 +50,14 @@ B200_PRM_I_UNROLL_FP64 = 38
 B200_PRM_I_UNROLL_FP32 = 39
 B200_PRM_I_KERNEL_TIMERS = 40
 B200_PRM_I_REFRESH_PERIOD = 41
+B200_PRM_I_WIDE_SLICES_FP64 = 42
+B200_PRM_I_WIDE_SLICES_FP32 = 43
 B200_PRM_R_REFRESH_DELTA = 30
 B200_PRM_R_TIME_H2D = 31
 B200_PRM_R_TIME_D2H = 32
 B200_PRM_R_TIME_LOOP = 33
+B200_PRM_R_SPMV_BYTES_FP64 = 34
+B200_PRM_R_SPMV_BYTES_FP32 = 35
 B200_PRM_R_TIME_KERNEL = 40
 STATUS_NAMES = {0: "ok", 1: "max_iter", 2: "breakdown", 3: "nonfinite", 4: "timeout", 5: "bad_input",
                 6: "cuda_error"}

@@ -394,11 +394,13 @@ std::vector<BatchItem> make_items(const BatchState& s, const BatchConfig& c) {
   return items;
 }
 
+// The batch kernel runs at 2 CTAs of 512 threads per SM (64 registers a
+// thread), so its rows take at most 3 slots in flight.
 template <class F>
 int dispatch_batch(int ndof, int u, F&& f) {
   return dispatch_ndof(ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
-    return dispatch_u(u, [&](auto Uc) {
+    return dispatch_u(u > 3 ? 3 : u, [&](auto Uc) {
       constexpr int U = eff_u(B, decltype(Uc)::value);
       return f(batch_cg_kernel<B, U>);
     });

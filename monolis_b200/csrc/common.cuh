@@ -37,6 +37,7 @@ __device__ __forceinline__ float axpy_rn(float a, float x, float y) { return fma
 __device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
 __device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
 __device__ __forceinline__ int ld_stream(const int* p) { return __ldcs(p); }
+__device__ __forceinline__ short ld_stream(const short* p) { return __ldcs(p); }
 
 // ---- deterministic one-pass grid reduction of K doubles, two levels.
 // Every block writes its K partial sums to partials[block*K + k]. Blocks are

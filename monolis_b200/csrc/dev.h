@@ -11,6 +11,14 @@
 // blocks in CSR (ascending column) order, which is the reference's summation
 // order. Padded slots (k >= row length) are never read: each thread stops at
 // its own row length, taken from the CSR offsets.
+//
+// Column ids are also kept compressed: for slot k of slice s, cbase[slptr[s]/32
+// + k] holds a base column c0 and col16[b] the 16-bit difference col[b] - c0 -
+// l, which is zero wherever the 32 rows of a slice have the same stencil (a
+// structured mesh) and small for any locally numbered mesh. A slice whose
+// differences do not all fit in 16 bits keeps reading col[]; slc[s] is
+// slptr[s] with bit 0 set for those slices. The compressed stream is 2 bytes
+// per block plus 4 bytes per slot per warp instead of 4 bytes per block.
 #pragma once
 
 #include <cstddef>
@@ -65,6 +73,17 @@ struct SellMatrix {
   long long padded2 = 0;
   long long* d_slptr2 = nullptr;  // nslices2+1, in blocks
   int* d_col2 = nullptr;
+  // compressed column ids (above) of both layouts; the paired layout has one
+  // base per slot of 64 rows and a pair of differences per lane:
+  // col = cbase2[slptr2[s]/64 + k] + 2l + h + col16p[slptr2[s] + 64k + 2l + h]
+  long long* d_slc = nullptr;
+  short* d_col16 = nullptr;
+  int* d_cbase = nullptr;
+  long long* d_slc2 = nullptr;
+  short* d_col16p = nullptr;
+  int* d_cbase2 = nullptr;
+  long long wide64 = 0, wide32 = 0;  // slices that keep 32-bit column ids
+  double bytes64 = 0, bytes32 = 0;   // HBM bytes of one SpMV in each layout
   // unroll depth (slots in flight per thread) picked by the autotuner
   int u64 = 2, u32 = 2;
   double* d_alu64 = nullptr;      // DIAG factors, entry-major: alu[e*N + row]
@@ -74,6 +93,7 @@ struct SellMatrix {
   double* d_csrval = nullptr;
   size_t cap_rowptr = 0, cap_slptr = 0, cap_col = 0, cap_val64 = 0, cap_val32 = 0;
   size_t cap_alu64 = 0, cap_alu32 = 0, cap_item = 0, cap_csrval = 0, cap_slptr2 = 0, cap_col2 = 0;
+  size_t cap_slc = 0, cap_col16 = 0, cap_cbase = 0, cap_slc2 = 0, cap_col16p = 0, cap_cbase2 = 0;
   bool have_val32 = false, have_alu = false, have_alu32 = false;
 };
 

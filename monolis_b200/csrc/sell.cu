@@ -100,6 +100,86 @@ __global__ void sell_fill_kernel(const int* __restrict__ rowptr, const int* __re
   }
 }
 
+// Compressed column ids of one layout, P rows per lane (P = 1: 32-row slices;
+// P = 2: the paired 64-row slices). One warp per slice. For slot position k,
+// with e = col - P*l - h over the real blocks of the slot, the base is the
+// midpoint c0 = min e + (max e - min e)/2 and every slot stores e - c0 in 16
+// bits, so a slot fits when its blocks span less than 65535 columns (beyond
+// the lane offset). On a structured mesh the rows at the two ends of a grid
+// line put neighbours one stencil position apart into the same slot; the
+// midpoint keeps those within range. A padded slot gets the difference of the
+// column clamp(c0 + P*l + h, 0, N-1), a valid column within 64 of c0 + P*l + h,
+// because the paired layout gathers at padded slots (their values are zero).
+// If any real slot of the slice does not fit, the slice is marked wide (bit 0
+// of slc) and keeps reading col[].
+// stats: [0] wide slices, [1] real blocks in wide slices, [2] slot positions
+// of compressed slices.
+template <int P>
+__global__ void col_compact_kernel(const int* __restrict__ rowptr, const long long* __restrict__ slptr, int N,
+                                   int nslices, const int* __restrict__ col, short* __restrict__ col16,
+                                   int* __restrict__ cbase, long long* __restrict__ slc,
+                                   unsigned long long* __restrict__ stats) {
+  constexpr int H = 32 * P;
+  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nslices) return;  // whole warps (blockDim is a multiple of 32)
+  const long long base = slptr[warp];
+  const int w = (int)((slptr[warp + 1] - base) / H);
+  int len[P];
+#pragma unroll
+  for (int h = 0; h < P; h++) {
+    const long long row = warp * H + P * lane + h;
+    len[h] = row < N ? rowptr[row + 1] - rowptr[row] : 0;
+  }
+  bool fit = true;
+  unsigned long long nreal = 0;
+  for (int k = 0; k < w; k++) {
+    const long long slot = base + (long long)k * H;
+    int c[P];
+    int emin = 0x7fffffff, emax = -0x7fffffff - 1;
+#pragma unroll
+    for (int h = 0; h < P; h++) {
+      c[h] = col[slot + P * lane + h];
+      if (k < len[h]) {
+        const int e = c[h] - P * lane - h;  // >= -63, < N
+        emin = min(emin, e);
+        emax = max(emax, e);
+      }
+    }
+    // some row of the slice is at least w long, so some lane has a real slot k
+    emin = __reduce_min_sync(0xffffffffu, emin);
+    emax = __reduce_max_sync(0xffffffffu, emax);
+    const long long c0 = (long long)emin + (((long long)emax - emin) >> 1);
+#pragma unroll
+    for (int h = 0; h < P; h++) {
+      const long long pos = (long long)P * lane + h;
+      long long d;
+      if (k < len[h]) {
+        d = (long long)c[h] - c0 - pos;
+        nreal++;
+      } else {
+        const long long tgt = c0 + pos < 0 ? 0 : (c0 + pos > N - 1 ? N - 1 : c0 + pos);
+        d = tgt - c0 - pos;
+      }
+      fit = fit && d >= -32768 && d <= 32767;
+      col16[slot + pos] = (short)d;
+    }
+    if (lane == 0) cbase[base / H + k] = (int)c0;
+  }
+  fit = __all_sync(0xffffffffu, fit);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) nreal += __shfl_xor_sync(0xffffffffu, nreal, o);
+  if (lane == 0) {
+    slc[warp] = base | (fit ? 0 : 1);
+    if (!fit) {
+      atomicAdd(&stats[0], 1ULL);
+      atomicAdd(&stats[1], nreal);
+    } else {
+      atomicAdd(&stats[2], (unsigned long long)w);
+    }
+  }
+}
+
 __global__ void to_fp32_kernel(const double* __restrict__ a, float* __restrict__ b, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     b[i] = (float)a[i];
@@ -206,6 +286,34 @@ __global__ void diag_apply_kernel(const double* __restrict__ alu, int N, const d
 }
 
 
+// Compressed column ids for one layout (P rows per lane); returns the column
+// bytes one SpMV streams: 2 per block and 4 per slot position in compressed
+// slices, 4 per block in wide slices.
+template <int P>
+int compact_columns(const SellMatrix& m, const long long* d_slptr, int nslices, long long padded,
+                    const int* d_col, short** col16, size_t& cap16, int** cbase, size_t& capb, long long** slc,
+                    size_t& capslc, long long& wide, double& col_bytes, cudaStream_t s) {
+  MB_CUDA_OK(grow(col16, cap16, (size_t)padded + 2));
+  MB_CUDA_OK(grow(cbase, capb, (size_t)(padded / (32 * P)) + 1));
+  MB_CUDA_OK(grow(slc, capslc, (size_t)nslices + 1));
+  unsigned long long* d_stats = nullptr;
+  MB_CUDA_OK(cudaMallocAsync((void**)&d_stats, 3 * sizeof(unsigned long long), s));
+  MB_CUDA_OK(cudaMemsetAsync(d_stats, 0, 3 * sizeof(unsigned long long), s));
+  if (nslices > 0) {
+    const long long threads = (long long)nslices * 32;
+    col_compact_kernel<P><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m.d_rowptr, d_slptr, m.N, nslices, d_col,
+                                                                          *col16, *cbase, *slc, d_stats);
+  }
+  unsigned long long st[3] = {0, 0, 0};
+  MB_CUDA_OK(cudaGetLastError());
+  MB_CUDA_OK(cudaMemcpyAsync(st, d_stats, sizeof(st), cudaMemcpyDeviceToHost, s));
+  MB_CUDA_OK(cudaStreamSynchronize(s));
+  cudaFreeAsync(d_stats, s);
+  wide = (long long)st[0];
+  col_bytes = 2.0 * (double)(m.nz - (long long)st[1]) + 4.0 * (double)st[1] + 4.0 * (double)st[2];
+  return kOk;
+}
+
 }  // namespace
 
 int sell_build(SellMatrix& m, const int* h_index, const int* h_item, const double* h_val, int N, int ndof,
@@ -269,6 +377,12 @@ int sell_layout(SellMatrix& m, cudaStream_t s) {
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
+  double col_bytes = 0;
+  rc = compact_columns<1>(m, m.d_slptr, nslices, m.padded, m.d_col, &m.d_col16, m.cap_col16, &m.d_cbase, m.cap_cbase,
+                          &m.d_slc, m.cap_slc, m.wide64, col_bytes, s);
+  if (rc) return rc;
+  // values, column ids, row offsets, slice offsets, x once and y
+  m.bytes64 = (double)m.nz * B2 * 8 + col_bytes + 4.0 * (N + 1) + 8.0 * nslices + 2.0 * N * ndof * 8;
   return sell_autotune(m, false, s);
 }
 
@@ -299,6 +413,11 @@ int sell_make_fp32(SellMatrix& m, cudaStream_t s) {
   });
   if (rc) return rc;
   MB_CUDA_OK(cudaGetLastError());
+  double col_bytes = 0;
+  rc = compact_columns<2>(m, m.d_slptr2, ns, m.padded2, m.d_col2, &m.d_col16p, m.cap_col16p, &m.d_cbase2,
+                          m.cap_cbase2, &m.d_slc2, m.cap_slc2, m.wide32, col_bytes, s);
+  if (rc) return rc;
+  m.bytes32 = (double)m.nz * B2 * 4 + col_bytes + 4.0 * (N + 1) + 8.0 * ns + 2.0 * N * m.ndof * 4;
   m.have_val32 = true;
   if (m.have_alu) {
     const long long na = (long long)m.N * m.ndof * m.ndof;
@@ -343,6 +462,12 @@ void sell_free(SellMatrix& m) {
   cudaFree(m.d_csrval);
   cudaFree(m.d_slptr2);
   cudaFree(m.d_col2);
+  cudaFree(m.d_slc);
+  cudaFree(m.d_col16);
+  cudaFree(m.d_cbase);
+  cudaFree(m.d_slc2);
+  cudaFree(m.d_col16p);
+  cudaFree(m.d_cbase2);
   m = SellMatrix();
 }
 

@@ -22,8 +22,10 @@ __device__ __forceinline__ T ldx(const T* p) {
 template <class V>
 struct SellView {
   const int* __restrict__ rowptr;
-  const long long* __restrict__ slptr;
+  const long long* __restrict__ slc;  // slice offset, bit 0 set: 32-bit column ids
   const int* __restrict__ col;
+  const short* __restrict__ col16;
+  const int* __restrict__ cbase;
   const V* __restrict__ val;
   int N;
 };
@@ -32,7 +34,23 @@ template <class V>
 inline SellView<V> view_of(const SellMatrix& m);
 template <>
 inline SellView<double> view_of<double>(const SellMatrix& m) {
-  return {m.d_rowptr, m.d_slptr, m.d_col, m.d_val64, m.N};
+  return {m.d_rowptr, m.d_slc, m.d_col, m.d_col16, m.d_cbase, m.d_val64, m.N};
+}
+
+// Column ids of slots k .. k+n-1 (n <= U) of one lane: 32-bit ids (wide
+// slice) or base + lane + 16-bit difference. The branch is uniform over the
+// warp (one slice).
+template <int U>
+__device__ __forceinline__ void load_cols(bool wide, const int* __restrict__ c, const short* __restrict__ c16,
+                                          const int* __restrict__ cb, int lane, int k, int n, int (&j)[U]) {
+  if (wide) {
+#pragma unroll
+    for (int u = 0; u < U; u++) j[u] = u < n ? ld_stream(c + (long long)(k + u) * kSlice) : 0;
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      j[u] = u < n ? __ldg(cb + k + u) + lane + (int)ld_stream(c16 + (long long)(k + u) * kSlice) : 0;
+  }
 }
 
 // y = (A x)[row] for one block row, blocks visited in CSR order. Within a
@@ -45,9 +63,13 @@ template <int B, int U, class V, class T, class XF>
 __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, int row, T (&y)[B]) {
   constexpr int B2 = B * B;
   const int lane = row & (kSlice - 1);
-  const long long base = A.slptr[row >> 5];
+  const long long sc = A.slc[row >> 5];
+  const long long base = sc & ~1LL;
+  const bool wide = sc & 1;
   const int len = A.rowptr[row + 1] - A.rowptr[row];
   const int* __restrict__ c = A.col + base + lane;
+  const short* __restrict__ c16 = A.col16 + base + lane;
+  const int* __restrict__ cb = A.cbase + (base >> 5);
   const V* __restrict__ v = A.val + base * B2 + lane;
 #pragma unroll
   for (int r = 0; r < B; r++) y[r] = T(0);
@@ -55,8 +77,7 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
   for (; k + U <= len; k += U) {
     int j[U];
     V a[U][B2];
-#pragma unroll
-    for (int u = 0; u < U; u++) j[u] = ld_stream(c + (long long)(k + u) * kSlice);
+    load_cols<U>(wide, c, c16, cb, lane, k, U, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -78,12 +99,11 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
   if (U > 1 && rem > 0) {
     int j[U];
     V a[U][B2];
+    load_cols<U>(wide, c, c16, cb, lane, k, rem, j);
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      j[u] = u < rem ? ld_stream(c + (long long)(k + u) * kSlice) : 0;
+    for (int u = 0; u < U; u++)
 #pragma unroll
       for (int e = 0; e < B2; e++) a[u][e] = u < rem ? ld_stream(v + ((long long)(k + u) * B2 + e) * kSlice) : V(0);
-    }
     T xs[U][B];
 #pragma unroll
     for (int u = 0; u < U; u++)
@@ -109,16 +129,42 @@ __device__ __forceinline__ void sell_row(const SellView<V>& A, const T* __restri
 // 2t+1 of the matrix; slot k of its pair is at block slptr2[t/32] + 64k + 2(t%32).
 struct SellView2 {
   const int* __restrict__ rowptr;
-  const long long* __restrict__ slptr2;
+  const long long* __restrict__ slc2;  // slice offset, bit 0 set: 32-bit column ids
   const int* __restrict__ col2;
+  const short* __restrict__ col16p;
+  const int* __restrict__ cbase2;
   const float* __restrict__ val;
   int N;
 };
 
-inline SellView2 view2_of(const SellMatrix& m) { return {m.d_rowptr, m.d_slptr2, m.d_col2, m.d_val32, m.N}; }
+inline SellView2 view2_of(const SellMatrix& m) {
+  return {m.d_rowptr, m.d_slc2, m.d_col2, m.d_col16p, m.d_cbase2, m.d_val32, m.N};
+}
 
 __device__ __forceinline__ float2 ld_stream2(const float2* p) { return __ldcs(p); }
 __device__ __forceinline__ int2 ld_stream2(const int2* p) { return __ldcs(p); }
+__device__ __forceinline__ short2 ld_stream2(const short2* p) { return __ldcs(p); }
+
+// Column ids of slots k .. k+n-1 of a row pair (paired layout).
+template <int U>
+__device__ __forceinline__ void load_cols2(bool wide, const int2* __restrict__ c, const short2* __restrict__ c16,
+                                           const int* __restrict__ cb, int lane2, int k, int n, int2 (&j)[U]) {
+  if (wide) {
+#pragma unroll
+    for (int u = 0; u < U; u++) j[u] = u < n ? ld_stream2(c + (long long)(k + u) * 32) : make_int2(0, 0);
+  } else {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      if (u < n) {
+        const int b = __ldg(cb + k + u) + lane2;
+        const short2 d = ld_stream2(c16 + (long long)(k + u) * 32);
+        j[u] = make_int2(b + d.x, b + 1 + d.y);
+      } else {
+        j[u] = make_int2(0, 0);
+      }
+    }
+  }
+}
 
 // y0/y1 = (A x) of rows 2t and 2t+1 in FP32 (fused multiply-add). Slots past
 // a row's length hold zero values and a valid column, so both rows run to the
@@ -130,11 +176,15 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   constexpr int B2 = B * B;
   const int r0 = 2 * t;
   const int lane2 = 2 * (t & 31);
-  const long long base = A.slptr2[t >> 5];
+  const long long sc = A.slc2[t >> 5];
+  const long long base = sc & ~1LL;
+  const bool wide = sc & 1;
   const int len0 = A.rowptr[r0 + 1] - A.rowptr[r0];
   const int len1 = (r0 + 1 < A.N) ? A.rowptr[r0 + 2] - A.rowptr[r0 + 1] : 0;
   const int len = len0 > len1 ? len0 : len1;
   const int2* __restrict__ c = reinterpret_cast<const int2*>(A.col2 + base + lane2);
+  const short2* __restrict__ c16 = reinterpret_cast<const short2*>(A.col16p + base + lane2);
+  const int* __restrict__ cb = A.cbase2 + (base >> 6);
   const float2* __restrict__ v = reinterpret_cast<const float2*>(A.val + base * B2 + lane2);
 #pragma unroll
   for (int r = 0; r < B; r++) { y0[r] = 0.f; y1[r] = 0.f; }
@@ -142,8 +192,7 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   for (; k + U <= len; k += U) {
     int2 j[U];
     float2 a[U][B2];
-#pragma unroll
-    for (int u = 0; u < U; u++) j[u] = ld_stream2(c + (long long)(k + u) * 32);
+    load_cols2<U>(wide, c, c16, cb, lane2, k, U, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -170,13 +219,12 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   if (rem > 0) {
     int2 j[U];
     float2 a[U][B2];
+    load_cols2<U>(wide, c, c16, cb, lane2, k, rem, j);
 #pragma unroll
-    for (int u = 0; u < U; u++) {
-      j[u] = u < rem ? ld_stream2(c + (long long)(k + u) * 32) : make_int2(0, 0);
+    for (int u = 0; u < U; u++)
 #pragma unroll
       for (int e = 0; e < B2; e++)
         a[u][e] = u < rem ? ld_stream2(v + ((long long)(k + u) * B2 + e) * 32) : make_float2(0.f, 0.f);
-    }
     float x0[U][B], x1[U][B];
 #pragma unroll
     for (int u = 0; u < U; u++)

@@ -62,6 +62,77 @@ def test_spmv_fp32_paired_layout(gpu, oracle, problem, kw):
     assert np.all(np.abs(y32 - y_ref) <= 1e-6 * bound + 1e-30)
 
 
+def _long_range_graph(n, n_far, seed):
+    """Chain 0-1-...-(n-1) plus n_far random edges between distant nodes:
+    slices holding a far edge need 32-bit column ids, the rest compress."""
+    rng = np.random.default_rng(seed)
+    chain = np.stack([np.arange(n - 1), np.arange(1, n)], axis=1)
+    far = np.stack([rng.integers(0, n // 4, n_far), rng.integers(3 * n // 4, n, n_far)], axis=1)
+    edges = np.ascontiguousarray(np.concatenate([chain, far]), dtype=np.int32)
+    vals = rng.standard_normal((len(edges), 4))
+    vals[:, 0] += 4.0
+    vals[:, 3] += 4.0
+    return edges, vals
+
+
+@pytest.mark.parametrize("n,n_far", [(200_003, 300), (70_001, 0)])
+def test_spmv_mixed_wide_and_compressed_slices(gpu, oracle, n, n_far):
+    """Column ids are stored as 16-bit differences per slice where they fit
+    and as 32-bit ids elsewhere; FP64 SpMV stays bit-identical to the oracle
+    on a matrix with both kinds of slices (and a last, partial slice), and
+    the FP32 paired layout stays within its rounding bound."""
+    import torch
+    edges, vals = _long_range_graph(n, n_far, seed=11)
+    ms = []
+    for lib in (gpu, oracle):
+        m = api.Monolis(lib)
+        m.get_nonzero_pattern_flat(n, 2, 1, edges)
+        m.add_elements(edges, 2, vals.reshape(-1), 4)
+        ms.append(m)
+    mp, mo = ms
+    mp.set_matrix_cache(True)
+    mp.set_precision(1)
+    mp.device_prepare()
+    wide64, wide32 = mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP64], mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP32]
+    if n_far:
+        assert 0 < wide64 < (n + 31) // 32 and 0 < wide32 < (n + 63) // 64
+    else:
+        assert wide64 == 0 and wide32 == 0
+    # the layout's byte count: 2-byte differences (+ bases) in compressed slices
+    nz = int(mo.csr_index()[-1])
+    full_bytes = nz * (8 + 4) + (n + 1) * 4 + 2 * n * 8
+    assert mp.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64] < full_bytes
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(n)
+    assert bits_equal(mp.matvec(x), mo.matvec(x))
+    x32 = x.astype(np.float32)
+    vals32 = mo.values().astype(np.float32).astype(np.float64)
+    mo.values()[:] = np.abs(vals32)
+    bound = mo.matvec(np.abs(x32.astype(np.float64)))
+    mo.values()[:] = vals32
+    y_ref = mo.matvec(x32.astype(np.float64))
+    d_x = torch.from_numpy(x32).cuda()
+    d_y = torch.empty_like(d_x)
+    mp.device_matvec(d_x.data_ptr(), d_y.data_ptr(), fp32=True)
+    torch.cuda.synchronize()
+    assert np.all(np.abs(d_y.cpu().numpy().astype(np.float64) - y_ref) <= 1e-6 * bound + 1e-30)
+
+
+def test_spmv_structured_grid_compresses(gpu, oracle):
+    """192^3 7-point grid: the rows at both ends of a grid line put stencil
+    neighbours +-n and +-n^2 into one slot; with the midpoint base every
+    slice still compresses, and the FP64 SpMV stays bit-identical."""
+    mp, b = build(gpu, "convection_diffusion", n=192, peclet=5.0)
+    mo, _ = build(oracle, "convection_diffusion", n=192, peclet=5.0)
+    mp.set_matrix_cache(True)
+    mp.set_precision(1)
+    mp.device_prepare()
+    assert mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP64] == 0
+    assert mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP32] == 0
+    x = np.random.default_rng(4).standard_normal(len(b))
+    assert bits_equal(mp.matvec(x), mo.matvec(x))
+
+
 def test_spmv_ndof2_random_blocks(gpu, oracle):
     # 10-node chain, ndof 2, like wrapper_test/solver/monolis_solver_c_test.c
     elem = np.array([[i, i + 1] for i in range(9)], dtype=np.int32)
