@@ -297,7 +297,7 @@ def batch_run(lib, systems, bs, label):
     cands = batch.autotune(iters=30)
     cfg = batch.config()
     out = {"systems": len(systems), "unknowns": int(sum(len(b) for b in bs)), "prepare_s": t_prep,
-           "config": {"cluster": cfg[0], "threads": cfg[1], "split_rows": cfg[2]},
+           "config": {"cluster": cfg[0], "threads": cfg[1], "split_rows": cfg[2], "unroll": batch.unroll()},
            "autotune": [{"cluster": c[0], "threads": c[1], "split_rows": c[2], "s": c[3]} for c in cands]}
     for name, tol, refine in (("refined_1e-8", 1e-8, True), ("fp32_1e-6", 1e-6, False)):
         xs, its, res, st = batch.solve(bs, tol=tol, max_iter=20000, refine=refine)  # warm-up; uploads b

@@ -179,6 +179,8 @@ int  monolis_b200_batch_add_csr(monolis_b200_batch* batch, int n, int ndof, cons
 int  monolis_b200_batch_prepare(monolis_b200_batch* batch, int precond, int autotune);
 int  monolis_b200_batch_set_config(monolis_b200_batch* batch, int cluster, int threads, long long split_rows);
 int  monolis_b200_batch_get_config(monolis_b200_batch* batch, int* cluster, int* threads, long long* split_rows);
+/* SpMV slots in flight per row of the batched kernel (1-3), picked by the autotuner */
+int  monolis_b200_batch_get_unroll(monolis_b200_batch* batch, int* unroll);
 /* re-times the candidates with `iters` iterations each and keeps the fastest;
  * on entry *n_candidates is the capacity of the output arrays, on return the
  * number of candidates timed */

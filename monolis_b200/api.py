@@ -179,6 +179,7 @@ _PRODUCT = {
     "monolis_b200_batch_prepare": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "monolis_b200_batch_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_longlong]),
     "monolis_b200_batch_get_config": (C.c_int, [C.c_void_p, _ip, _ip, C.POINTER(C.c_longlong)]),
+    "monolis_b200_batch_get_unroll": (C.c_int, [C.c_void_p, _ip]),
     "monolis_b200_batch_autotune": (C.c_int, [C.c_void_p, C.c_int, _ip, _ip, _ip, C.POINTER(C.c_longlong), _dp]),
     "monolis_b200_batch_solve_R": (C.c_int, [C.c_void_p, C.POINTER(_dp), C.POINTER(_dp), C.c_double, C.c_int,
                                              C.c_int, _ip, _dp, _ip]),
@@ -606,6 +607,11 @@ class Batch:
         c, t, sp = C.c_int(), C.c_int(), C.c_longlong()
         _check(self.lib.monolis_b200_batch_get_config(self.h, C.byref(c), C.byref(t), C.byref(sp)), "batch_config")
         return c.value, t.value, sp.value
+
+    def unroll(self):
+        u = C.c_int()
+        _check(self.lib.monolis_b200_batch_get_unroll(self.h, C.byref(u)), "batch_unroll")
+        return u.value
 
     def autotune(self, iters=30, cap=64):
         n = C.c_int(cap)

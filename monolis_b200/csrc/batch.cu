@@ -49,6 +49,10 @@ namespace {
 
 constexpr int kBatchMaxThreads = 512;
 constexpr int kBatchRowAlign = 64;
+// The batched kernel is latency-bound (small systems, cluster barriers every
+// phase), so it reads the 32-bit column ids: the 16-bit form's extra base load
+// per slot cost more than its bytes save (C4: 0.165 s vs 0.144 s).
+constexpr bool kBatchCols16 = false;
 
 struct BatchSys {
   long long row0;  // first block row in the stacked matrix (multiple of 64)
@@ -162,7 +166,7 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
     v[0] = v[1] = 0.0;
     for (long long row = rlo + tid; row < rhi; row += nt) {
       double ax[B];
-      sell_row_f<B, U, double, double>(a.A64, XPlusYCoherent{a.x, a.y}, (int)row, ax);
+      sell_row_f<B, U, double, double, kBatchCols16>(a.A64, XPlusYCoherent{a.x, a.y}, (int)row, ax);
       float t[B], w[B];
 #pragma unroll
       for (int c = 0; c < B; c++) {
@@ -208,7 +212,7 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
       double w[1] = {0.0};
       for (long long t = plo + tid; t < phi; t += nt) {
         float q0[B], q1[B];
-        sell_row2<B, U, true>(a.A32, a.p, (int)t, q0, q1);
+        sell_row2<B, U, true, kBatchCols16>(a.A32, a.p, (int)t, q0, q1);
 #pragma unroll
         for (int c = 0; c < B; c++) {
           const long long i0 = 2 * t * B + c, i1 = (2 * t + 1) * B + c;
@@ -324,6 +328,7 @@ cudaError_t dalloc(P** p, size_t n) {
 struct BatchConfig {
   int cluster = 0, threads = 0;
   long long split_rows = 0;
+  int unroll = 0;  // SpMV slots in flight (0: the matrix's autotuned depth, at most 3)
 };
 
 struct BatchState {
@@ -401,7 +406,7 @@ int dispatch_batch(int ndof, int u, F&& f) {
   return dispatch_ndof(ndof, [&](auto Bc) {
     constexpr int B = decltype(Bc)::value;
     return dispatch_u(u > 3 ? 3 : u, [&](auto Uc) {
-      constexpr int U = eff_u(B, decltype(Uc)::value);
+      constexpr int U = eff_u(B, decltype(Uc)::value > 3 ? 3 : decltype(Uc)::value);
       return f(batch_cg_kernel<B, U>);
     });
   });
@@ -419,7 +424,7 @@ int build_graph(BatchState* s, const BatchConfig& c, const BatchArgs& args0) {
     cudaGraphExecDestroy(s->exec);
     s->exec = nullptr;
   }
-  return dispatch_batch(s->ndof, s->A.u32, [&](auto kernel) -> int {
+  return dispatch_batch(s->ndof, c.unroll > 0 ? c.unroll : s->A.u32, [&](auto kernel) -> int {
     if (c.cluster > 8)
       MB_CUDA_OK(cudaFuncSetAttribute(kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
@@ -578,7 +583,7 @@ int batch_set_config(BatchState* s, int cluster, int threads, long long split_ro
   if (cluster < 1 || cluster > 16 || (cluster & (cluster - 1)) || threads < 64 || threads > kBatchMaxThreads ||
       threads % 32)
     return kBadInput;
-  BatchConfig c{cluster, threads, split_rows};
+  BatchConfig c{cluster, threads, split_rows, s->cfg.unroll};
   s->cfg = c;
   if (s->exec) {
     cudaGraphExecDestroy(s->exec);
@@ -597,7 +602,8 @@ int batch_solve_device(BatchState* s, double tol, int max_iter, int refine, doub
 }
 
 // Times each candidate configuration on the batch (right-hand side b = 1,
-// `iters` iterations) and keeps the fastest.
+// `iters` iterations) and keeps the fastest; then, at that configuration,
+// the SpMV unroll depth 1, 2 or 3.
 int batch_autotune(BatchState* s, int iters, std::vector<std::pair<BatchConfig, double>>* log) {
   if (!s->prepared) return kBadInput;
   const size_t n = (size_t)s->nrows * s->ndof;
@@ -620,6 +626,20 @@ int batch_autotune(BatchState* s, int iters, std::vector<std::pair<BatchConfig, 
   BatchConfig bc{};
   int rc = kOk;
   for (const BatchConfig& c : cand) {
+    s->cfg = c;
+    double t0 = 0.0, t1 = 0.0;
+    rc = batch_solve_device(s, 0.0, iters, 0, 0.0, &t0);  // warm
+    if (!rc) rc = batch_solve_device(s, 0.0, iters, 0, 0.0, &t1);
+    if (rc) break;
+    if (log) log->push_back({c, t1});
+    if (t1 < best) {
+      best = t1;
+      bc = c;
+    }
+  }
+  for (int u = 1; u <= 3 && rc == kOk && bc.cluster > 0; u++) {
+    BatchConfig c = bc;
+    c.unroll = u;
     s->cfg = c;
     double t0 = 0.0, t1 = 0.0;
     rc = batch_solve_device(s, 0.0, iters, 0, 0.0, &t0);  // warm
@@ -706,6 +726,13 @@ int monolis_b200_batch_get_config(monolis_b200_batch* b, int* cluster, int* thre
   if (cluster) *cluster = b->s.cfg.cluster;
   if (threads) *threads = b->s.cfg.threads;
   if (split_rows) *split_rows = b->s.cfg.split_rows;
+  return MONOLIS_B200_OK;
+}
+
+int monolis_b200_batch_get_unroll(monolis_b200_batch* b, int* unroll) {
+  if (!b || !b->s.prepared || !unroll) return MONOLIS_B200_BAD_INPUT;
+  const int u = b->s.cfg.unroll > 0 ? b->s.cfg.unroll : b->s.A.u32;
+  *unroll = u > 3 ? 3 : u;
   return MONOLIS_B200_OK;
 }
 

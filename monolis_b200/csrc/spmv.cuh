@@ -58,14 +58,15 @@ __device__ __forceinline__ void load_cols(bool wide, const int* __restrict__ c, 
 // (src/linalg/matvec.f90:805-823); the FP64 instantiation keeps exactly that
 // sequence of roundings. U slots are loaded before any is consumed so that
 // each thread keeps U*(B*B + 1) independent loads in flight.
-// xf(i) gives entry i = column*B + l of the multiplied vector.
-template <int B, int U, class V, class T, class XF>
+// xf(i) gives entry i = column*B + l of the multiplied vector. kCols16 =
+// false reads the 32-bit column ids of every slice.
+template <int B, int U, class V, class T, bool kCols16 = true, class XF>
 __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, int row, T (&y)[B]) {
   constexpr int B2 = B * B;
   const int lane = row & (kSlice - 1);
   const long long sc = A.slc[row >> 5];
   const long long base = sc & ~1LL;
-  const bool wide = sc & 1;
+  const bool wide = !kCols16 || (sc & 1);
   const int len = A.rowptr[row + 1] - A.rowptr[row];
   const int* __restrict__ c = A.col + base + lane;
   const short* __restrict__ c16 = A.col16 + base + lane;
@@ -171,14 +172,14 @@ __device__ __forceinline__ void load_cols2(bool wide, const int2* __restrict__ c
 // longer length.
 // The entries of the multiplied vector come from xf(i) (i = column*B + l):
 // a plain gather, or a value computed from other vectors (see sell_row2).
-template <int B, int U, class XF>
+template <int B, int U, bool kCols16 = true, class XF>
 __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int t, float (&y0)[B], float (&y1)[B]) {
   constexpr int B2 = B * B;
   const int r0 = 2 * t;
   const int lane2 = 2 * (t & 31);
   const long long sc = A.slc2[t >> 5];
   const long long base = sc & ~1LL;
-  const bool wide = sc & 1;
+  const bool wide = !kCols16 || (sc & 1);
   const int len0 = A.rowptr[r0 + 1] - A.rowptr[r0];
   const int len1 = (r0 + 1 < A.N) ? A.rowptr[r0 + 2] - A.rowptr[r0 + 1] : 0;
   const int len = len0 > len1 ? len0 : len1;
@@ -247,10 +248,10 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   }
 }
 
-template <int B, int U, bool kCoherent = false>
+template <int B, int U, bool kCoherent = false, bool kCols16 = true>
 __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
                                           float (&y1)[B]) {
-  sell_row2_f<B, U>(A, [&](long long i) { return ldx<kCoherent>(x + i); }, t, y0, y1);
+  sell_row2_f<B, U, kCols16>(A, [&](long long i) { return ldx<kCoherent>(x + i); }, t, y0, y1);
 }
 
 // 16-byte vector type of an element type.
