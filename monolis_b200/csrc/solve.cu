@@ -344,10 +344,11 @@ __global__ void shard_cg_kernel(SolverState* st, double* hist) {
   if (st->done || (st->iter % st->iter_rr) == 0) return;
   fin_cg(st, st->red[0], st->red[1], hist);
 }
-__global__ void shard_resid_kernel(SolverState* st, double* hist) {
+__global__ void shard_resid_kernel(SolverState* st, double* hist, int mode) {
   if (st->done || !(st->iter == 0 || st->rr_flag)) return;
   st->rr_flag = 0;
-  fin_cg(st, st->red[0], st->red[1], hist);
+  if (mode == 0) fin_cg(st, st->red[0], st->red[1], hist);
+  else fin_bicg(st, st->red[0], st->red[1], hist);
 }
 
 // ---------------------------------------------------------------------------
@@ -453,6 +454,10 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // alpha after the all-reduce (shard_bicg_alpha_kernel)
+      st->red[0] = tot[0];
+      return;
+    }
     st->c2 = tot[0];
     if (tot[0] == 0.0) { st->done = 1; st->status = kBreakdown; return; }
     st->alpha = st->rho / tot[0];
@@ -517,6 +522,11 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // omega after the all-reduce (shard_bicg_omega_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
     st->ts = tot[0];
     st->tt = tot[1];
     st->omega = tot[1] == 0.0 ? 0.0 : tot[0] / tot[1];
@@ -578,9 +588,32 @@ __global__ void __launch_bounds__(kThreads)
     return;
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (!Mixed && st->sharded) {  // fin_bicg after the all-reduce (shard_bicg_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
     if (Mixed) fin_mixed_bicg(st, tot[0], tot[1], hist);
     else fin_bicg(st, tot[0], tot[1], hist);
   });
+}
+
+// Multi-rank BiCGSTAB: the scalar steps with the all-reduced sums in red[].
+__global__ void shard_bicg_alpha_kernel(SolverState* st) {
+  if (st->done) return;
+  st->c2 = st->red[0];
+  if (st->red[0] == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+  st->alpha = st->rho / st->red[0];
+}
+__global__ void shard_bicg_omega_kernel(SolverState* st) {
+  if (st->done) return;
+  st->ts = st->red[0];
+  st->tt = st->red[1];
+  st->omega = st->red[1] == 0.0 ? 0.0 : st->red[0] / st->red[1];
+}
+__global__ void shard_bicg_kernel(SolverState* st, double* hist) {
+  if (st->done || (st->iter % st->iter_rr) == 0) return;
+  fin_bicg(st, st->red[0], st->red[1], hist);
 }
 
 // ---------------------------------------------------------------------------
@@ -977,6 +1010,7 @@ struct Plan {
   std::function<void(cudaStream_t, cudaEvent_t*, bool special)> iteration;
   std::function<void(cudaStream_t)> finalize;  // mixed: final fold
   int kernels = 0;         // kernel slots of an iteration (FP64: the last is the special kernel)
+  int launches = 0, launches_special = 0;  // kernels of an iteration, if not one per slot (multi-rank)
   bool always_all = false; // every slot launches every iteration (mixed)
   std::vector<int> kind;   // per slot: 0 SpMV, 1 other vector kernel, 2 precond-applying kernel
 };
@@ -996,8 +1030,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
   if (p.method != 1 && p.method != 5) return kBadInput;
-  if (p.shard && (p.method != 1 || p.precision != 0 || p.np_rows < N)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG\n");
+  if (p.shard && (p.precision != 0 || p.np_rows < N)) {
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG or BiCGSTAB\n");
     return kBadInput;
   }
   // vectors gathered by the SpMV hold the ghost rows too
@@ -1068,9 +1102,12 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         int rc2 = shard_halo(*sp, x, s);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
         if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
-        shard_resid_kernel<<<1, 1, 0, s>>>(st, hist);
+        shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 0);
         if (rc2) return rc2;
+        const int hk = (sp->n_send > 0) + (sp->n_recv > 0);  // pack / unpack kernels of a halo update
         plan.kernels = 5;
+        plan.launches = 5 + hk;
+        plan.launches_special = 6 + 2 * hk;
         plan.kind = {1, 0, 2, 1, 0};
         plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
           if (ev) cudaEventRecord(ev[0], ss);
@@ -1092,7 +1129,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
             shard_halo(*sp, x, ss);
             k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
             shard_allreduce(*sp, st->red, 2, ss);
-            shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist);
+            shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist, 0);
           }
           if (ev) cudaEventRecord(ev[5], ss);
         };
@@ -1116,6 +1153,63 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           if (special) k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket,
                                                              st, hist);
           if (ev) cudaEventRecord(ev[4], ss);
+        };
+      } else if (p.shard) {
+        // multi-rank BiCGSTAB: halo updates of PT and ST before the products,
+        // all-reduced dots (alpha, omega, the residual norms)
+        const ShardPlan* sp = p.shard;
+        double *r = vec.get<double>(n), *rt = vec.get<double>(n), *pp = vec.get<double>(n),
+               *pt = vec.get<double>(n_ext), *sv = vec.get<double>(n), *stv = vec.get<double>(n_ext),
+               *t = vec.get<double>(n), *vv = vec.get<double>(n);
+        if (!r || !rt || !pp || !pt || !sv || !stv || !t || !vv) return kCudaError;
+        if (cudaMemsetAsync(pt, 0, sizeof(double) * n_ext, s) != cudaSuccess ||
+            cudaMemsetAsync(stv, 0, sizeof(double) * n_ext, s) != cudaSuccess)
+          return kCudaError;
+        auto k_v = bicg_v_kernel<B, U, double, double>;
+        auto k_t = bicg_t_kernel<B, U, double, double>;
+        auto k_xr = bicg_xr_kernel<B, double>;
+        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
+        const int g_p = pgrid(bicg_p_kernel<B, double>), g_s = pgrid(bicg_s_kernel<B, double>);
+        int rc2 = shard_halo(*sp, x, s);
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
+        if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+        shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 1);
+        if (rc2) return rc2;
+        const int hk = (sp->n_send > 0) + (sp->n_recv > 0);
+        plan.kernels = 6;
+        plan.launches = 8 + 2 * hk;
+        plan.launches_special = 10 + 3 * hk;
+        plan.kind = {2, 0, 2, 0, 1, 0};
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          bicg_p_kernel<B, double><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          shard_halo(*sp, pt, ss);
+          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
+          shard_allreduce(*sp, st->red, 1, ss);
+          shard_bicg_alpha_kernel<<<1, 1, 0, ss>>>(st);
+          if (ev) cudaEventRecord(ev[2], ss);
+          bicg_s_kernel<B, double><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
+          if (ev) cudaEventRecord(ev[3], ss);
+          shard_halo(*sp, stv, ss);
+          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
+          shard_allreduce(*sp, st->red, 2, ss);
+          shard_bicg_omega_kernel<<<1, 1, 0, ss>>>(st);
+          if (ev) cudaEventRecord(ev[4], ss);
+          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+          if (!special) {
+            shard_allreduce(*sp, st->red, 2, ss);
+            shard_bicg_kernel<<<1, 1, 0, ss>>>(st, hist);
+          }
+          if (ev) cudaEventRecord(ev[5], ss);
+          if (special) {
+            shard_halo(*sp, x, ss);
+            k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st,
+                                                 hist);
+            shard_allreduce(*sp, st->red, 2, ss);
+            shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist, 1);
+          }
+          if (ev) cudaEventRecord(ev[6], ss);
         };
       } else {
         double *r = vec.get<double>(n), *rt = vec.get<double>(n), *pp = vec.get<double>(n),
@@ -1221,6 +1315,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   MB_CUDA_OK(cudaGetLastError());
   long long launched_kernels = 1;
   auto kernels_of = [&](bool special) -> long long {
+    if (plan.launches > 0) return special ? plan.launches_special : plan.launches;
     return plan.kernels - ((special || plan.always_all) ? 0 : 1);
   };
 

@@ -2,8 +2,10 @@
 monolis_b200.partition builds rank-local systems and MONOLIS_COM halo tables
 whose halo exchange (pack send_item -> neighbour -> unpack into recv_item)
 and per-rank dot products, followed by the scalar updates the device code
-applies (FP64 CG with block-Jacobi), reproduce the single-rank solve of the
-oracle: same solution to 1e-10, iteration count within 2."""
+applies (FP64 CG and BiCGSTAB with block-Jacobi: halo updates of the
+multiplied vectors P, PT, ST and X, all-reduced sums for every dot),
+reproduce the single-rank solve of the oracle: same solution, iteration
+count within 2."""
 import os
 import sys
 
@@ -22,7 +24,12 @@ def global_system(problem):
     from monolis_b200 import problems as P
     lib = api.load_library(ORACLE, oracle=True)
     m = api.Monolis(lib)
-    b = P.laplacian(m, n=7) if problem == "laplacian" else P.elasticity(m, n=5)
+    if problem == "laplacian":
+        b = P.laplacian(m, n=7)
+    elif problem == "convection_diffusion":
+        b = P.convection_diffusion(m, n=8, peclet=5.0)
+    else:
+        b = P.elasticity(m, n=5)
     return m, np.ascontiguousarray(b)
 
 
@@ -37,7 +44,7 @@ def local_matvec(p, nd, x):
     return y.reshape(-1)
 
 
-def _worker(rank, world, port, problem, q):
+def _worker(rank, world, port, problem, q, method="cg"):
     import torch
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -87,6 +94,10 @@ def _worker(rank, world, port, problem, q):
         x = np.zeros(npr * nd)
         halo(x)
         r = bl[:n * nd] - local_matvec(p, nd, x)
+        if method == "bicgstab":
+            it = _bicgstab(r, x, p, nd, n, npr, halo, gdot, prec)
+            q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
+            return
         z = prec(r)
         B2 = gdot(bl, bl)
         rho = gdot(r, z)
@@ -108,6 +119,75 @@ def _worker(rank, world, port, problem, q):
         q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
     finally:
         dist.destroy_process_group()
+
+
+def _bicgstab(r, x, p, nd, n, npr, halo, gdot, prec):
+    """BiCGSTAB of the device code's multi-rank plan (src/iterative/BiCGSTAB.f90:87-170):
+    PT and ST get their ghost entries before each product; every dot is a
+    local sum followed by an all-reduce. Returns the iteration count."""
+    rt = r.copy()
+    B2 = gdot(r, r)
+    rho = gdot(r, rt)
+    pv = np.zeros(n * nd)
+    vv = np.zeros(n * nd)
+    pt = np.zeros(npr * nd)
+    st = np.zeros(npr * nd)
+    alpha = omega = 1.0
+    for it in range(1, 5000):
+        if it == 1:
+            pv = r.copy()
+        else:
+            beta = (rho / rho1) * (alpha / omega)
+            pv = r + beta * (pv - omega * vv)
+        pt[:n * nd] = prec(pv)
+        halo(pt)
+        vv = local_matvec(p, nd, pt)
+        alpha = rho / gdot(rt, vv)
+        s = r - alpha * vv
+        st[:n * nd] = prec(s)
+        halo(st)
+        t = local_matvec(p, nd, st)
+        ts, tt = gdot(t, s), gdot(t, t)
+        omega = ts / tt if tt != 0.0 else 0.0
+        x[:n * nd] += alpha * pt[:n * nd] + omega * st[:n * nd]
+        r = s - omega * t
+        rr = gdot(r, r)
+        if np.sqrt(rr / B2) < 1e-8:
+            return it
+        rho1, rho = rho, gdot(r, rt)
+    return 5000
+
+
+def _run_ranks(problem, world, method, port):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, problem, q, method)) for r in range(world)]
+    for p_ in procs:
+        p_.start()
+    out = [q.get(timeout=180) for _ in range(world)]
+    for p_ in procs:
+        p_.join(timeout=60)
+        assert p_.exitcode == 0
+    return out
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_partitioned_bicgstab_matches_single_rank(world, oracle):
+    from monolis_b200 import api
+    from helpers import solve
+    m, b = global_system("convection_diffusion")
+    x_ref, it_ref, _, st = solve(m, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=1e-8)
+    assert st == 0
+    out = _run_ranks("convection_diffusion", world, "bicgstab", 32700 + (os.getpid() % 2000) + 11 * world)
+    x = np.zeros_like(b)
+    its = set()
+    for rank, glob, xl, it in out:
+        x[np.array(glob)] = xl
+        its.add(it)
+    assert len(its) == 1  # every rank stops at the same iteration
+    assert abs(its.pop() - it_ref) <= 2
+    x_tight, _, _, _ = solve(m, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=1e-12)
+    assert np.linalg.norm(x - x_tight) / np.linalg.norm(x_tight) < 1e-6
 
 
 @pytest.mark.parametrize("problem,world", [("laplacian", 2), ("laplacian", 3), ("elasticity", 2)])

@@ -1,8 +1,9 @@
 """The multi-rank device path (halo updates through NCCL, dot products summed
-by an NCCL all-reduce, scalar updates in a separate one-thread kernel) run
-with a one-rank communicator: it must give exactly the bits and iteration
-count of the single-rank solve, also past the true-residual replacement at
-iteration 200. (Runs here have one GPU; more ranks cannot share it.)"""
+by an NCCL all-reduce, scalar updates in separate one-thread kernels), FP64
+CG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
+bits and iteration count of the single-rank solve, also past the
+true-residual replacement at iteration 200. (Runs here have one GPU; more
+ranks cannot share it.)"""
 import numpy as np
 import pytest
 
@@ -13,12 +14,22 @@ from helpers import bits_equal, build, solve
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("problem,kw", [("elasticity", dict(n=8)), ("elasticity", dict(n=24)),
-                                        ("laplacian", dict(n=20))])
-def test_sharded_path_one_rank_bit_identical(gpu, problem, kw):
+@pytest.mark.parametrize("problem,kw,method,rr", [
+    ("elasticity", dict(n=8), api.ITER_CG, 0),
+    ("elasticity", dict(n=24), api.ITER_CG, 0),
+    ("laplacian", dict(n=20), api.ITER_CG, 0),
+    ("convection_diffusion", dict(n=16, peclet=5.0), api.ITER_BICGSTAB, 0),
+    ("convection_diffusion", dict(n=16, peclet=0.5), api.ITER_BICGSTAB, 7),
+    ("laplacian", dict(n=24), api.ITER_BICGSTAB, 5),
+    ("elasticity", dict(n=10), api.ITER_BICGSTAB, 0),
+])
+def test_sharded_path_one_rank_bit_identical(gpu, problem, kw, method, rr):
+    """rr > 0: true residual every rr iterations (instead of 200), so the
+    replacement step of the multi-rank plan runs several times."""
     mp, b = build(gpu, problem, **kw)
     nd = mp.NDOF
-    xp, itp, resp, stp = solve(mp, b, api.ITER_CG, api.PREC_DIAG, tol=1e-8)
+    mp.Iarray[api.B200_PRM_I_ITER_RR] = rr
+    xp, itp, resp, stp = solve(mp, b, method, api.PREC_DIAG, tol=1e-8)
     assert stp == 0
     p = partition.partition_rows(mp.csr_index(), mp.csr_item() - 1, mp.values(), nd, 1)[0]
     assert p["N"] == p["NP"] == mp.N
@@ -28,12 +39,15 @@ def test_sharded_path_one_rank_bit_identical(gpu, problem, kw):
     ms.set_error_abort(False)
     ms.set_halo(p, 0, 1)
     ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
-    xs, its, ress, sts = solve(ms, b, api.ITER_CG, api.PREC_DIAG, tol=1e-8)
+    ms.Iarray[api.B200_PRM_I_ITER_RR] = rr
+    xs, its, ress, sts = solve(ms, b, method, api.PREC_DIAG, tol=1e-8)
     assert sts == 0
     assert its == itp and ress == resp
     assert bits_equal(xs, xp)
-    if kw.get("n") == 24:
+    if problem == "elasticity" and kw.get("n") == 24:
         assert itp > 200  # crosses the true-residual replacement
+    if rr:
+        assert itp > 2 * rr
     ms.finalize()
 
 
@@ -46,6 +60,6 @@ def test_sharded_path_rejects_unsupported(gpu):
     ms.set_error_abort(False)
     ms.set_halo(p, 0, 1)
     ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
-    _, _, _, st = solve(ms, b, api.ITER_BICGSTAB, api.PREC_DIAG)
-    assert st == 5  # the multi-rank solve is FP64 CG
+    _, _, _, st = solve(ms, b, api.ITER_CG, api.PREC_DIAG, precision=1)
+    assert st == 5  # the multi-rank solve is FP64 (CG or BiCGSTAB)
     ms.finalize()
