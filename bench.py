@@ -343,6 +343,33 @@ def workload_c4(lib, args):
     return res
 
 
+def workload_c4_sharded(lib, args, rank, world):
+    """C4's independent systems over the ranks: replicas with no data-path
+    collective (monolis_b200.partition.split_systems, greedy by stored
+    blocks); every rank solves its share in one batch, FP32-refined to 1e-8;
+    the job time is the max over ranks."""
+    from monolis_b200 import partition
+    sides = problems.batch_sides(args.c4_count)
+    share = partition.split_systems([7 * int(s) ** 3 for s in sides], world)[rank]
+    systems = [problems.fv_diffusion_csr(int(sides[i]), 4000 + i) for i in share]
+    bs = [problems.uniform(5000 + i, int(sides[i]) ** 3) for i in share]
+    batch = api.Batch(lib)
+    for ix, it, v, _ in systems:
+        batch.add_csr(len(ix) - 1, 1, ix, it, v)
+    batch.prepare(precond=api.PREC_DIAG, autotune=True)
+    batch.solve(bs, tol=1e-8, max_iter=20000, refine=True)  # warm-up; uploads b
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    _, _, st = batch.device_solve(tol=1e-8, max_iter=20000, refine=True)
+    t = batch.last_seconds()
+    batch.destroy()
+    return {"workload": f"{len(sides)} C4 systems over {world} ranks (greedy by stored blocks), FP32-refined 1e-8",
+            "systems_this_rank": len(share), "unknowns_this_rank": int(sum(len(b) for b in bs)),
+            "all_converged_this_rank": bool(np.all(st == 0)),
+            "s": max_over_ranks(t, world), "scaling": "strong (the 512 systems are split)"}
+
+
 def multi_rhs_run(lib, sysm, rhs):
     """All right-hand sides in one persistent kernel (matrix read once per
     iteration for all of them): FP32-refined to 1e-8 and FP64 to 1e-8."""
@@ -554,6 +581,9 @@ def main():
     ap.add_argument("--workloads", default="c3,c4,c5",
                     help="secondary workloads to run after the headline (any of c3,c4,c5, or none)")
     ap.add_argument("--c4-count", type=int, default=512)
+    ap.add_argument("--c4-sharded", action="store_true",
+                    help="the C4 systems split over the N ranks (greedy by stored blocks), each rank "
+                         "solving its share in one batch, max over ranks (N = 1: the whole batch)")
     ap.add_argument("--c4-rhs-side", type=int, default=96)
     ap.add_argument("--c4-rhs", type=int, default=32)
     ap.add_argument("--c3-n", type=int, default=256)
@@ -747,6 +777,11 @@ def main():
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
     workloads = {}
+    if args.c4_sharded:
+        try:
+            workloads["c4_sharded"] = workload_c4_sharded(lib, args, rank, world)
+        except Exception as e:  # report, do not hide
+            workloads["c4_sharded"] = {"failed": repr(e)}
     if rank == 0 and world == 1:
         for w in [w for w in args.workloads.split(",") if w and w != "none"]:
             try:

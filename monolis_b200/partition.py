@@ -77,3 +77,20 @@ def partition_rows(index, item, val, ndof, nranks):
                  recv_item=np.array(recv_item, dtype=np.int32), send_pe=np.array(send_pe, dtype=np.int32),
                  send_index=np.array(send_index, dtype=np.int32), send_item=np.array(send_item, dtype=np.int32))
     return parts
+
+
+def split_systems(nnz, nranks):
+    """Independent systems (batched solve) over ranks, no communication:
+    greedy longest-processing-time assignment by stored blocks -- systems in
+    decreasing nnz order, each to the rank with the smallest load so far (ties
+    to the lower rank). Returns one ascending list of system indices per rank;
+    the largest load is at most 4/3 of the optimum (Graham's bound)."""
+    nnz = np.asarray(nnz, dtype=np.int64)
+    order = np.argsort(-nnz, kind="stable")
+    load = np.zeros(nranks, dtype=np.int64)
+    out = [[] for _ in range(nranks)]
+    for i in order:
+        r = int(np.argmin(load))
+        out[r].append(int(i))
+        load[r] += nnz[i]
+    return [sorted(o) for o in out]
