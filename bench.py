@@ -367,7 +367,7 @@ def workload_c4_sharded(lib, args, rank, world):
     return {"workload": f"{len(sides)} C4 systems over {world} ranks (greedy by stored blocks), FP32-refined 1e-8",
             "systems_this_rank": len(share), "unknowns_this_rank": int(sum(len(b) for b in bs)),
             "all_converged_this_rank": bool(np.all(st == 0)),
-            "s": max_over_ranks(t, world), "scaling": "strong (the 512 systems are split)"}
+            "s": max_over_ranks(t, world), "scaling": f"strong (the {len(sides)} systems are split)"}
 
 
 def multi_rhs_run(lib, sysm, rhs):
