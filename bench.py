@@ -806,6 +806,23 @@ def main():
             "spmv_fp32_in_solve_gbs": spmv32_bytes / kt32[1] / 1e9,
             "spmv_fp64_in_solve_gbs": spmv64_bytes / kt64[1] / 1e9,
         }
+        # solver roofline: the minimum fused CG schedule per iteration, {SpMV + <p,q>},
+        # {x (y), r update, z = M^-1 r, <r,z>, <r,r>}, {p = z + beta p}: the SpMV bytes +
+        # 12 vector passes + the block-Jacobi factors (9 per block row); the refined
+        # solver adds its FP64 refreshes (FP64 SpMV + x, y, b, r, z and the factors)
+        it_mixed = int(np.median(iters))
+        bytes_it64 = spmv64_bytes + 12 * n_unk * 8 + 9 * N * 8
+        bytes_it32 = spmv32_bytes + 12 * n_unk * 4 + 9 * N * 4
+        bytes_refresh = spmv64_bytes + n_unk * (8 + 4 + 8 + 4 + 4) + 9 * N * 4
+        total32 = it_mixed * bytes_it32 + nref * bytes_refresh
+        solver_roofline = {
+            "fp64": {"bytes_per_iteration": bytes_it64, "iterations": it64,
+                     "achieved_gbs": it64 * bytes_it64 / t64_max / 1e9,
+                     "frac_of_measured": it64 * bytes_it64 / t64_max / 1e9 / peak},
+            "mixed": {"bytes_per_iteration": bytes_it32, "bytes_per_refresh": bytes_refresh, "refreshes": nref,
+                      "iterations": it_mixed, "achieved_gbs": total32 / t_mixed_max / 1e9,
+                      "frac_of_measured": total32 / t_mixed_max / 1e9 / peak},
+        }
         line = {
             "metric": METRIC, "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3, "higher_is_better": False,
@@ -832,6 +849,7 @@ def main():
                                    "average launch inside a mixed solve, kernel-timer mode",
                          "algorithmic_bytes_per_launch": spmv32_bytes, "peak_kind": peak_kind},
             "in_solve_kernels": in_solve,
+            "solver_roofline": solver_roofline,
             "spmv_layout": layout,
             "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call",
