@@ -35,7 +35,14 @@ from monolis_b200 import api, problems  # noqa: E402
 
 ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libmonolis_oracle.so")
 FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_iterations.json")
-METRIC = "time to rel.res 1e-8, FP32-refined block-CSR CG (3D elasticity 128^3 nodes, ndof=3)"
+def metric_name(n):
+    """The headline metric, shared by both arms (the arithmetic is in `dtype`)."""
+    return f"time to rel.res 1e-8, block-CSR CG (3D elasticity {n}^3 nodes, ndof=3)"
+
+
+def workload_name(n, nz):
+    return (f"3D linear elasticity {n}^3 nodes, hex8 Q1, E=1 nu=0.3, ndof=3, {nz} 3x3 blocks, "
+            f"CG + 3x3 block-Jacobi, rel.res 1e-8")
 TOL = 1e-8
 # DRAM bytes (read + write) per launch of cg_spmv2_kernel divided by its
 # layout bytes, from the ncu --set full capture at 64^3 nodes
@@ -554,12 +561,12 @@ def run_reference(args, rank):
     iters = it_full if it_full else None
     value = t_iter * iters if iters else None
     line = {
-        "impl": "reference", "metric": METRIC.replace("FP32-refined", "FP64 CPU oracle"), "value": value,
+        "impl": "reference", "metric": metric_name(args.n), "value": value,
         "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3 if value else None, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"3D elasticity {args.n}^3 nodes hex8 ndof=3, CG+DIAG, rel.res 1e-8",
-                   "parallelism": "cpu"},
+        "config": {"workload": workload_name(args.n, int(m.csr_index()[-1])), "unknowns": int(len(b)),
+                   "nz_blocks": int(m.csr_index()[-1]), "parallelism": f"cpu, {threads} threads (oracle, FP64)"},
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
                          "sample": f"{sample_iters} CG iterations per step (median of {args.steps}), "
                                    f"extrapolated x {iters} iterations (oracle count for this system)"},
@@ -824,11 +831,10 @@ def main():
                       "frac_of_measured": total32 / t_mixed_max / 1e9 / peak},
         }
         line = {
-            "metric": METRIC, "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "metric": metric_name(args.n), "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
-            "config": {"workload": f"3D linear elasticity {args.n}^3 nodes, hex8 Q1, E=1 nu=0.3, ndof=3, "
-                                   f"{nz} 3x3 blocks, CG + 3x3 block-Jacobi, rel.res 1e-8",
+            "config": {"workload": workload_name(args.n, nz),
                        "unknowns": n_unk, "nz_blocks": nz, "padded_blocks": padded,
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (matrix 4.2 GB FP64 + 2.2 GB FP32)"},
