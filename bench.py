@@ -676,6 +676,7 @@ def main():
     torch.cuda.nvtx.range_pop()
     barrier()
     clocks = clk.summary()
+    nref = int(m.Iarray[api.B200_PRM_I_N_REFINE])  # FP64 refreshes of the last timed solve
     # per-kernel durations inside a solve (kernel-timer mode, one extra solve
     # of each precision, after the timed steps)
     x_mixed = d_x.clone()
@@ -685,7 +686,6 @@ def main():
     m.set_precision(1)
     d_x.copy_(x_mixed)
     t_mixed = float(np.mean(times))
-    nref = int(m.Iarray[api.B200_PRM_I_N_REFINE])
     err_vs_fp64 = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
     # true FP64 residual of the mixed solution (device FP64 SpMV)
     d_r = torch.empty_like(d_x)
