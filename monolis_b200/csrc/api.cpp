@@ -937,13 +937,14 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   if (!rc) rc = ensure_vec(s, n);
   if (!rc && sharded) {
     mb::ShardTables t;
+    t.rank = com->my_rank;
     t.send_pe.assign(com->send_neib_pe, com->send_neib_pe + com->send_n_neib);
     t.send_ptr.assign(com->send_index, com->send_index + com->send_n_neib + 1);
     t.send_item.assign(com->send_item, com->send_item + (com->send_n_neib ? com->send_index[com->send_n_neib] : 0));
     t.recv_pe.assign(com->recv_neib_pe, com->recv_neib_pe + com->recv_n_neib);
     t.recv_ptr.assign(com->recv_index, com->recv_index + com->recv_n_neib + 1);
     t.recv_item.assign(com->recv_item, com->recv_item + (com->recv_n_neib ? com->recv_index[com->recv_n_neib] : 0));
-    rc = mb::shard_setup(s->shard, t, m->mat.NDOF);
+    rc = mb::shard_setup(s->shard, t, m->mat.NDOF, s->A, ctx().stream);
     s->shard.comm = ncomm;
   }
   if (rc) {

@@ -144,24 +144,36 @@ int element_gradient64(int n_elem, int n_base, int ndof, const int* elem, const 
 // Halo tables of one rank: for every neighbour, the local block rows it sends
 // (send_item, 0-based) or receives into (recv_item, ghost rows), with offsets.
 struct ShardTables {
+  int rank = 0;  // this rank (a neighbour entry equal to it is a local copy)
   std::vector<int> send_pe, send_ptr, send_item, recv_pe, recv_ptr, recv_item;
 };
 struct ShardPlan {
   void* comm = nullptr;  // ncclComm_t
-  int ndof = 0;
+  int ndof = 0, rank = 0;
   std::vector<int> send_pe, recv_pe, send_ptr, recv_ptr;
   long long n_send = 0, n_recv = 0;
   int* d_send_item = nullptr;
   int* d_recv_item = nullptr;
   void* d_sendbuf = nullptr;
   void* d_recvbuf = nullptr;
+  // 32-row slices of the device matrix: those whose rows read no ghost entry
+  // (interior) first, then the others (boundary); the interior product runs
+  // while the halo update is in flight on `side`
+  int* d_slices = nullptr;
+  int n_int = 0, n_bnd = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 int shard_unique_id(void* out128);
 int shard_comm_create(void** comm, const void* id128, int rank, int size);
 void shard_comm_destroy(void* comm);
-int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof);
+int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof, const SellMatrix& A, cudaStream_t s);
 void shard_free(ShardPlan& sp);
 int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s);
+// halo update of v on the side stream, ordered after the work already on s;
+// shard_halo_join makes s wait for it
+int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s);
+int shard_halo_join(const ShardPlan& sp, cudaStream_t s);
 int shard_allreduce(const ShardPlan& sp, double* d, int k, cudaStream_t s);
 
 struct SolveParams {

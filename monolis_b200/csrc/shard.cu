@@ -5,11 +5,15 @@
 // sums the dot products over the ranks).
 //
 // Here the halo update is a pack kernel, NCCL send/receive pairs with every
-// neighbour inside one NCCL group, and an unpack kernel; a dot product is the
+// neighbour inside one NCCL group (a neighbour entry naming this rank itself
+// is a device copy), and an unpack kernel; a dot product is the
 // device-resident local sum followed by an NCCL all-reduce and a one-thread
-// kernel that applies the scalar update with the global sums. Everything is
-// enqueued on the solver stream, so it is captured in the solver's CUDA
-// graphs like the rest of the iteration. Every rank evaluates the scalar
+// kernel that applies the scalar update with the global sums. Before the
+// products of the iteration the halo update runs on a side stream while the
+// solver stream multiplies the interior slices (rows that read no ghost
+// entry); the boundary slices follow once the update has landed. Everything
+// is enqueued on the solver stream or forked from it with events, so it is
+// captured in the solver's CUDA graphs like the rest of the iteration. Every rank evaluates the scalar
 // recurrences from the same all-reduced bits, so all ranks stop at the same
 // iteration and issue the same sequence of collectives.
 //
@@ -100,6 +104,21 @@ __global__ void unpack_kernel(T* __restrict__ v, const int* __restrict__ item, l
   }
 }
 
+// Flag per 32-row slice: 1 when one of its rows reads a ghost entry
+// (block column >= N, the ghost rows following the owned ones).
+__global__ void boundary_slices_kernel(const int* __restrict__ rowptr, const int* __restrict__ item, int N,
+                                       int nslices, int* __restrict__ flag) {
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long sl = gt >> 5;
+  if (sl >= nslices) return;  // whole warps (blockDim is a multiple of 32)
+  const long long row = gt;   // slice sl, lane gt & 31
+  bool ghost = false;
+  if (row < N)
+    for (int j = rowptr[row]; j < rowptr[row + 1]; j++) ghost = ghost || (item[j] - 1 >= N);
+  const unsigned any = __ballot_sync(0xffffffffu, ghost);
+  if ((gt & 31) == 0) flag[sl] = any != 0;
+}
+
 }  // namespace
 
 int shard_unique_id(void* out128) {
@@ -128,8 +147,9 @@ void shard_comm_destroy(void* comm) {
   if (comm && nccl().loaded) nccl().CommDestroy(static_cast<ncclComm_t>(comm));
 }
 
-int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof) {
+int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof, const SellMatrix& A, cudaStream_t s) {
   sp.ndof = ndof;
+  sp.rank = t.rank;
   sp.send_pe = t.send_pe;
   sp.recv_pe = t.recv_pe;
   sp.send_ptr = t.send_ptr;
@@ -153,6 +173,45 @@ int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof) {
   sp.d_sendbuf = sp.d_recvbuf = nullptr;
   MB_CUDA_OK(cudaMalloc(&sp.d_sendbuf, sizeof(double) * (ns * ndof + 2)));
   MB_CUDA_OK(cudaMalloc(&sp.d_recvbuf, sizeof(double) * (nr * ndof + 2)));
+  // a neighbour entry naming this rank exchanges with itself: the matching
+  // send and receive lists must have the same length
+  for (size_t q = 0; q < t.send_pe.size(); q++) {
+    if (t.send_pe[q] != t.rank) continue;
+    bool ok = false;
+    for (size_t r = 0; r < t.recv_pe.size(); r++)
+      if (t.recv_pe[r] == t.rank)
+        ok = t.recv_ptr[r + 1] - t.recv_ptr[r] == t.send_ptr[q + 1] - t.send_ptr[q];
+    if (!ok) {
+      fprintf(stderr, "** monolis_b200: halo tables: the self-exchange lists differ in length\n");
+      return kBadInput;
+    }
+  }
+  // interior / boundary slices of the device matrix
+  const int nsl = A.nslices;
+  std::vector<int> flag(nsl > 0 ? nsl : 1, 0);
+  int* d_flag = nullptr;
+  MB_CUDA_OK(cudaMalloc((void**)&d_flag, sizeof(int) * (nsl + 1)));
+  if (nsl > 0) {
+    const long long threads = (long long)nsl * 32;
+    boundary_slices_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(A.d_rowptr, A.d_item, A.N, nsl, d_flag);
+    MB_CUDA_OK(cudaGetLastError());
+    MB_CUDA_OK(cudaMemcpyAsync(flag.data(), d_flag, sizeof(int) * nsl, cudaMemcpyDeviceToHost, s));
+  }
+  MB_CUDA_OK(cudaStreamSynchronize(s));
+  cudaFree(d_flag);
+  std::vector<int> order;
+  order.reserve(nsl);
+  for (int i = 0; i < nsl; i++)
+    if (!flag[i]) order.push_back(i);
+  sp.n_int = (int)order.size();
+  for (int i = 0; i < nsl; i++)
+    if (flag[i]) order.push_back(i);
+  sp.n_bnd = nsl - sp.n_int;
+  rc = up_int(&sp.d_slices, order);
+  if (rc) return rc;
+  if (!sp.side) MB_CUDA_OK(cudaStreamCreateWithFlags(&sp.side, cudaStreamNonBlocking));
+  if (!sp.ev_fork) MB_CUDA_OK(cudaEventCreateWithFlags(&sp.ev_fork, cudaEventDisableTiming));
+  if (!sp.ev_join) MB_CUDA_OK(cudaEventCreateWithFlags(&sp.ev_join, cudaEventDisableTiming));
   return kOk;
 }
 
@@ -161,6 +220,10 @@ void shard_free(ShardPlan& sp) {
   cudaFree(sp.d_recv_item);
   cudaFree(sp.d_sendbuf);
   cudaFree(sp.d_recvbuf);
+  cudaFree(sp.d_slices);
+  if (sp.side) cudaStreamDestroy(sp.side);
+  if (sp.ev_fork) cudaEventDestroy(sp.ev_fork);
+  if (sp.ev_join) cudaEventDestroy(sp.ev_join);
   sp = ShardPlan();
 }
 
@@ -171,14 +234,30 @@ int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) {
   double* sb = static_cast<double*>(sp.d_sendbuf);
   double* rb = static_cast<double*>(sp.d_recvbuf);
   if (sp.n_send > 0) pack_kernel<double><<<148 * 2, 256, 0, s>>>(v, sp.d_send_item, sp.n_send, nd, sb);
-  if (sp.n_send > 0 || sp.n_recv > 0) {
+  // the list this rank sends to itself lands directly in its receive buffer
+  for (size_t q = 0; q < sp.send_pe.size(); q++) {
+    if (sp.send_pe[q] != sp.rank) continue;
+    for (size_t r = 0; r < sp.recv_pe.size(); r++) {
+      if (sp.recv_pe[r] != sp.rank) continue;
+      const size_t cnt = (size_t)(sp.send_ptr[q + 1] - sp.send_ptr[q]) * nd;
+      if (cnt)
+        MB_CUDA_OK(cudaMemcpyAsync(rb + (size_t)sp.recv_ptr[r] * nd, sb + (size_t)sp.send_ptr[q] * nd,
+                                   cnt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+  }
+  bool remote = false;
+  for (int pe : sp.send_pe) remote = remote || pe != sp.rank;
+  for (int pe : sp.recv_pe) remote = remote || pe != sp.rank;
+  if (remote) {
     int rc = nccl_check(a.GroupStart(), "ncclGroupStart");
     for (size_t q = 0; !rc && q < sp.send_pe.size(); q++) {
+      if (sp.send_pe[q] == sp.rank) continue;
       const size_t off = (size_t)sp.send_ptr[q] * nd, cnt = (size_t)(sp.send_ptr[q + 1] - sp.send_ptr[q]) * nd;
       rc = nccl_check(a.Send(sb + off, cnt, ncclDouble, sp.send_pe[q], static_cast<ncclComm_t>(sp.comm), s),
                       "ncclSend");
     }
     for (size_t q = 0; !rc && q < sp.recv_pe.size(); q++) {
+      if (sp.recv_pe[q] == sp.rank) continue;
       const size_t off = (size_t)sp.recv_ptr[q] * nd, cnt = (size_t)(sp.recv_ptr[q + 1] - sp.recv_ptr[q]) * nd;
       rc = nccl_check(a.Recv(rb + off, cnt, ncclDouble, sp.recv_pe[q], static_cast<ncclComm_t>(sp.comm), s),
                       "ncclRecv");
@@ -188,6 +267,19 @@ int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) {
   }
   if (sp.n_recv > 0) unpack_kernel<double><<<148 * 2, 256, 0, s>>>(v, sp.d_recv_item, sp.n_recv, nd, rb);
   MB_CUDA_OK(cudaGetLastError());
+  return kOk;
+}
+
+int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s) {
+  MB_CUDA_OK(cudaEventRecord(sp.ev_fork, s));
+  MB_CUDA_OK(cudaStreamWaitEvent(sp.side, sp.ev_fork, 0));
+  const int rc = shard_halo(sp, v, sp.side);
+  MB_CUDA_OK(cudaEventRecord(sp.ev_join, sp.side));
+  return rc;
+}
+
+int shard_halo_join(const ShardPlan& sp, cudaStream_t s) {
+  MB_CUDA_OK(cudaStreamWaitEvent(s, sp.ev_join, 0));
   return kOk;
 }
 

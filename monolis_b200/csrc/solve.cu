@@ -70,6 +70,35 @@ int pgrid(K kernel) {
   return g;
 }
 
+// Rows a matrix kernel visits: all N (slices == nullptr), or the 32-row
+// slices listed (multi-rank: interior or boundary slices). Returns the row
+// of work item i, or -1 past the matrix end.
+struct RowSet {
+  const int* __restrict__ slices;
+  int nsl;
+  __device__ __forceinline__ long long count(int N) const { return slices ? (long long)nsl * kSlice : N; }
+  __device__ __forceinline__ int row(long long i, int N) const {
+    const long long r = slices ? (long long)slices[i >> 5] * kSlice + (i & (kSlice - 1)) : i;
+    return r < N ? (int)r : -1;
+  }
+};
+
+// body(row) for this thread's rows of a grid-stride loop: all N rows, or
+// (kSet) the rows of the listed slices.
+template <bool kSet, class F>
+__device__ __forceinline__ void for_rows(const RowSet& rs, int N, F&& body) {
+  if constexpr (kSet) {
+    const long long nit = rs.count(N);
+    for (long long it = blockIdx.x * (long long)blockDim.x + threadIdx.x; it < nit;
+         it += (long long)gridDim.x * blockDim.x) {
+      const int row = rs.row(it, N);
+      if (row >= 0) body(row);
+    }
+  } else {
+    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) body(row);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Scalar updates run by the last block of a grid reduction.
 // ---------------------------------------------------------------------------
@@ -208,13 +237,13 @@ __global__ void cg_p_kernel(long long n, T* __restrict__ p, const T* __restrict_
 }
 
 // Q = A P fused with omega = <P,Q>, alpha = rho/omega (CG.f90:85-87).
-template <int B, int U, class V, class T>
+template <int B, int U, class V, class T, bool kSet = false>
 __global__ void __launch_bounds__(kThreads)
     cg_spmv_kernel(SellView<V> A, const T* __restrict__ p, T* __restrict__ q, double* partials,
-                   unsigned int* ticket, SolverState* st) {
+                   unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
   double v[1] = {0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+  for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, p, row, y);
 #pragma unroll
@@ -223,10 +252,10 @@ __global__ void __launch_bounds__(kThreads)
       q[i] = y[c];
       v[0] += (double)p[i] * (double)y[c];
     }
-  }
+  });
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
-    if (st->sharded) {
-      st->red[0] = tot[0];
+    if (st->sharded) {  // acc: the boundary slices add to the interior ones' sum
+      st->red[0] = acc ? st->red[0] + tot[0] : tot[0];
       return;
     }
     st->omega = tot[0];
@@ -437,13 +466,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // V = A PT; c2 = <RT,V>; alpha = rho/c2 (BiCGSTAB.f90:113-123)
-template <int B, int U, class V, class T>
+template <int B, int U, class V, class T, bool kSet = false>
 __global__ void __launch_bounds__(kThreads)
     bicg_v_kernel(SellView<V> A, const T* __restrict__ pt, T* __restrict__ vv, const T* __restrict__ rt,
-                  double* partials, unsigned int* ticket, SolverState* st) {
+                  double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
   double v[1] = {0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+  for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, pt, row, y);
 #pragma unroll
@@ -452,10 +481,10 @@ __global__ void __launch_bounds__(kThreads)
       vv[i] = y[c];
       v[0] += (double)rt[i] * (double)y[c];
     }
-  }
+  });
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
-    if (st->sharded) {  // alpha after the all-reduce (shard_bicg_alpha_kernel)
-      st->red[0] = tot[0];
+    if (st->sharded) {  // alpha after the all-reduce (shard_bicg_alpha_kernel); acc as cg_spmv
+      st->red[0] = acc ? st->red[0] + tot[0] : tot[0];
       return;
     }
     st->c2 = tot[0];
@@ -504,13 +533,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // T = A ST; (T,S), (T,T); omega = (T,S)/(T,T) or 0 (BiCGSTAB.f90:128-146)
-template <int B, int U, class V, class T>
+template <int B, int U, class V, class T, bool kSet = false>
 __global__ void __launch_bounds__(kThreads)
     bicg_t_kernel(SellView<V> A, const T* __restrict__ stv, T* __restrict__ t, const T* __restrict__ s,
-                  double* partials, unsigned int* ticket, SolverState* st) {
+                  double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
   double v[2] = {0.0, 0.0};
-  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+  for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, stv, row, y);
 #pragma unroll
@@ -520,11 +549,11 @@ __global__ void __launch_bounds__(kThreads)
       v[0] += (double)y[c] * (double)s[i];
       v[1] += (double)y[c] * (double)y[c];
     }
-  }
+  });
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
-    if (st->sharded) {  // omega after the all-reduce (shard_bicg_omega_kernel)
-      st->red[0] = tot[0];
-      st->red[1] = tot[1];
+    if (st->sharded) {  // omega after the all-reduce (shard_bicg_omega_kernel); acc as cg_spmv
+      st->red[0] = acc ? st->red[0] + tot[0] : tot[0];
+      st->red[1] = acc ? st->red[1] + tot[1] : tot[1];
       return;
     }
     st->ts = tot[0];
@@ -1096,7 +1125,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
                *pp = vec.get<double>(n_ext);
         if (!r || !z || !q || !pp) return kCudaError;
         if (cudaMemsetAsync(pp, 0, sizeof(double) * n_ext, s) != cudaSuccess) return kCudaError;
-        auto k_spmv = cg_spmv_kernel<B, U, double, double>;
+        auto k_spmv = cg_spmv_kernel<B, U, double, double, true>;
         auto k_upd = cg_update_kernel<B, double>;
         const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
         int rc2 = shard_halo(*sp, x, s);
@@ -1105,16 +1134,22 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 0);
         if (rc2) return rc2;
         const int hk = (sp->n_send > 0) + (sp->n_recv > 0);  // pack / unpack kernels of a halo update
+        const int nb = sp->n_bnd > 0;                         // boundary-slice product
+        const RowSet rs_int{sp->d_slices, sp->n_int}, rs_bnd{sp->d_slices + sp->n_int, sp->n_bnd};
+        const int g_bnd = std::max(1, std::min(g_spmv, (int)(((long long)sp->n_bnd * kSlice + kThreads - 1) / kThreads)));
         plan.kernels = 5;
-        plan.launches = 5 + hk;
-        plan.launches_special = 6 + 2 * hk;
+        plan.launches = 5 + hk + nb;
+        plan.launches_special = 6 + 2 * hk + nb;
         plan.kind = {1, 0, 2, 1, 0};
         plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
           if (ev) cudaEventRecord(ev[0], ss);
           cg_p_kernel<double><<<gvec, kThreads, 0, ss>>>(n, pp, z, st);
           if (ev) cudaEventRecord(ev[1], ss);
-          shard_halo(*sp, pp, ss);
-          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st);
+          // interior rows while the halo update is in flight, then the boundary rows
+          shard_halo_fork(*sp, pp, ss);
+          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st, rs_int, 0);
+          shard_halo_join(*sp, ss);
+          if (nb) k_spmv<<<g_bnd, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st, rs_bnd, 1);
           shard_allreduce(*sp, st->red, 1, ss);
           shard_alpha_kernel<<<1, 1, 0, ss>>>(st);
           if (ev) cudaEventRecord(ev[2], ss);
@@ -1146,7 +1181,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           if (ev) cudaEventRecord(ev[0], ss);
           cg_p_kernel<double><<<gvec, kThreads, 0, ss>>>(n, pp, z, st);
           if (ev) cudaEventRecord(ev[1], ss);
-          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st);
+          k_spmv<<<g_spmv, kThreads, 0, ss>>>(A64, pp, q, partials, ticket, st, RowSet{nullptr, 0}, 0);
           if (ev) cudaEventRecord(ev[2], ss);
           k_upd<<<g_upd, kThreads, 0, ss>>>(N, x, pp, r, q, z, alu, prec, partials, ticket, st, hist);
           if (ev) cudaEventRecord(ev[3], ss);
@@ -1165,8 +1200,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (cudaMemsetAsync(pt, 0, sizeof(double) * n_ext, s) != cudaSuccess ||
             cudaMemsetAsync(stv, 0, sizeof(double) * n_ext, s) != cudaSuccess)
           return kCudaError;
-        auto k_v = bicg_v_kernel<B, U, double, double>;
-        auto k_t = bicg_t_kernel<B, U, double, double>;
+        auto k_v = bicg_v_kernel<B, U, double, double, true>;
+        auto k_t = bicg_t_kernel<B, U, double, double, true>;
         auto k_xr = bicg_xr_kernel<B, double>;
         const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
         const int g_p = pgrid(bicg_p_kernel<B, double>), g_s = pgrid(bicg_s_kernel<B, double>);
@@ -1176,23 +1211,32 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 1);
         if (rc2) return rc2;
         const int hk = (sp->n_send > 0) + (sp->n_recv > 0);
+        const int nb = sp->n_bnd > 0;
+        const RowSet rs_int{sp->d_slices, sp->n_int}, rs_bnd{sp->d_slices + sp->n_int, sp->n_bnd};
+        const long long bnd_blocks = ((long long)sp->n_bnd * kSlice + kThreads - 1) / kThreads;
+        const int gb_v = std::max(1, (int)std::min<long long>(g_v, bnd_blocks));
+        const int gb_t = std::max(1, (int)std::min<long long>(g_t, bnd_blocks));
         plan.kernels = 6;
-        plan.launches = 8 + 2 * hk;
-        plan.launches_special = 10 + 3 * hk;
+        plan.launches = 8 + 2 * hk + 2 * nb;
+        plan.launches_special = 10 + 3 * hk + 2 * nb;
         plan.kind = {2, 0, 2, 0, 1, 0};
         plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
           if (ev) cudaEventRecord(ev[0], ss);
           bicg_p_kernel<B, double><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
           if (ev) cudaEventRecord(ev[1], ss);
-          shard_halo(*sp, pt, ss);
-          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
+          shard_halo_fork(*sp, pt, ss);
+          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st, rs_int, 0);
+          shard_halo_join(*sp, ss);
+          if (nb) k_v<<<gb_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st, rs_bnd, 1);
           shard_allreduce(*sp, st->red, 1, ss);
           shard_bicg_alpha_kernel<<<1, 1, 0, ss>>>(st);
           if (ev) cudaEventRecord(ev[2], ss);
           bicg_s_kernel<B, double><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
           if (ev) cudaEventRecord(ev[3], ss);
-          shard_halo(*sp, stv, ss);
-          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
+          shard_halo_fork(*sp, stv, ss);
+          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st, rs_int, 0);
+          shard_halo_join(*sp, ss);
+          if (nb) k_t<<<gb_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st, rs_bnd, 1);
           shard_allreduce(*sp, st->red, 2, ss);
           shard_bicg_omega_kernel<<<1, 1, 0, ss>>>(st);
           if (ev) cudaEventRecord(ev[4], ss);
@@ -1228,11 +1272,11 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           if (ev) cudaEventRecord(ev[0], ss);
           bicg_p_kernel<B, double><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu, prec, st);
           if (ev) cudaEventRecord(ev[1], ss);
-          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st);
+          k_v<<<g_v, kThreads, 0, ss>>>(A64, pt, vv, rt, partials, ticket, st, RowSet{nullptr, 0}, 0);
           if (ev) cudaEventRecord(ev[2], ss);
           bicg_s_kernel<B, double><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu, prec, st);
           if (ev) cudaEventRecord(ev[3], ss);
-          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st);
+          k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st, RowSet{nullptr, 0}, 0);
           if (ev) cudaEventRecord(ev[4], ss);
           k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
           if (ev) cudaEventRecord(ev[5], ss);

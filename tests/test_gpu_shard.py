@@ -63,3 +63,56 @@ def test_sharded_path_rejects_unsupported(gpu):
     _, _, _, st = solve(ms, b, api.ITER_CG, api.PREC_DIAG, precision=1)
     assert st == 5  # the multi-rank solve is FP64 (CG or BiCGSTAB)
     ms.finalize()
+
+
+@pytest.mark.parametrize("problem,kw,method", [
+    ("laplacian", dict(n=14), api.ITER_CG),
+    ("elasticity", dict(n=7), api.ITER_CG),
+    ("convection_diffusion", dict(n=14, peclet=5.0), api.ITER_BICGSTAB),
+])
+def test_sharded_boundary_rows_through_self_halo(gpu, problem, kw, method):
+    """A one-rank system whose rows read some columns through ghost entries:
+    every 7th node gets a ghost copy, filled by a halo list the rank sends to
+    itself. The rows that read a ghost form the boundary slices, multiplied
+    after the halo update while the interior slices run beside it; the
+    solution must match the plain solve (the rows' sums run in a different
+    order, so to the solver tolerance, not bit for bit)."""
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    N = mp.N
+    x_ref, it_ref, _, st = solve(mp, b, method, api.PREC_DIAG, tol=1e-12)
+    assert st == 0
+    index = mp.csr_index().astype(np.int64)
+    item = (mp.csr_item() - 1).astype(np.int64)
+    val = mp.values().reshape(-1, nd * nd)
+    mirrored = np.arange(3, N, 7)
+    ghost = np.full(N, -1, dtype=np.int64)
+    ghost[mirrored] = N + np.arange(len(mirrored))
+    NP = N + len(mirrored)
+    new_index, new_item, new_val = [0], [], []
+    for i in range(N):
+        cols = item[index[i]:index[i + 1]]
+        cols2 = np.where((ghost[cols] >= 0) & (cols != i), ghost[cols], cols)
+        order = np.argsort(cols2, kind="stable")
+        new_item.extend(cols2[order].tolist())
+        new_val.append(val[index[i]:index[i + 1]][order])
+        new_index.append(len(new_item))
+    new_index += [new_index[-1]] * (NP - N)  # ghost rows hold no blocks
+    new_val = np.concatenate(new_val).reshape(-1)
+    assert any(c >= N for c in new_item)
+    halo = {"N": N, "recv_pe": [0], "recv_index": [0, len(mirrored)], "recv_item": np.arange(N, NP),
+            "send_pe": [0], "send_index": [0, len(mirrored)], "send_item": mirrored}
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(N, NP, nd, len(new_item), new_val, np.array(new_index, dtype=np.int32),
+                       np.array(new_item, dtype=np.int32))
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_halo(halo, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    bl = np.zeros(NP * nd)
+    bl[:N * nd] = b
+    xs, its, _, sts = solve(ms, bl, method, api.PREC_DIAG, tol=1e-12)
+    assert sts == 0
+    assert abs(its - it_ref) <= 2, (its, it_ref)
+    assert np.linalg.norm(xs[:N * nd] - x_ref) / np.linalg.norm(x_ref) < 1e-9
+    ms.finalize()
