@@ -28,6 +28,12 @@ import time
 
 import numpy as np
 
+# OpenMP threads of the host assembly and of the CPU baseline sleep between
+# parallel regions instead of spinning, so they do not take the cores the
+# solver's host loop (graph launches, state reads) runs on. Set before any
+# library that links the OpenMP runtime is loaded.
+os.environ.setdefault("OMP_WAIT_POLICY", "PASSIVE")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
