@@ -1436,9 +1436,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         cudaGraphDestroy(graph);
       }
     }
-    cudaEvent_t ev[2];
-    cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
-    cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+    // Three launches in flight: the host reads the state word of the oldest
+    // while two more batches keep the GPU busy, so a late host thread (a busy
+    // core) does not leave the device idle. After the verdict the batches
+    // still queued return at kernel entry.
+    constexpr int kInFlight = 3;
+    cudaEvent_t ev[kInFlight];
+    for (auto& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
     long long next = cur.iter;  // iteration the next enqueued batch starts with (batches start at 1 mod batch)
     int inflight = 0, slot = 0;
     while (err == cudaSuccess) {
@@ -1454,9 +1458,9 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       next += batch;
       cudaMemcpyAsync(&sc.h_st[slot], sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
       cudaEventRecord(ev[slot], s);
-      slot ^= 1;
-      if (++inflight < 2) continue;
-      err = cudaEventSynchronize(ev[slot]);  // the older launch
+      slot = (slot + 1) % kInFlight;
+      if (++inflight < kInFlight) continue;
+      err = cudaEventSynchronize(ev[slot]);  // the oldest launch (its slot is reused next)
       if (err != cudaSuccess) break;
       inflight--;
       if (sc.h_st[slot].done) break;
@@ -1467,8 +1471,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     }
     cudaError_t e2 = cudaStreamSynchronize(s);
     if (err == cudaSuccess) err = e2;
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
+    for (auto& e : ev) cudaEventDestroy(e);
     for (auto& e : exec)
       if (e) cudaGraphExecDestroy(e);
     if (err != cudaSuccess) return report_cuda(err, "solver loop", __FILE__, __LINE__);
