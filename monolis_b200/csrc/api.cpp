@@ -536,8 +536,13 @@ void print_summary(MONOLIS* m) {
 bool method_supported(const MONOLIS* m) {
   const int mth = m->prm.Iarray[MONOLIS_PRM_I_METHOD];
   const int pc = m->prm.Iarray[MONOLIS_PRM_I_PRECOND];
-  if (mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB) {
-    fprintf(stderr, "** monolis_b200: solver %s is not provided by this library (CG, BiCGSTAB)\n", str_iter(mth));
+  if (mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG) {
+    fprintf(stderr, "** monolis_b200: solver %s is not provided by this library (CG, PipeCG, BiCGSTAB)\n",
+            str_iter(mth));
+    return false;
+  }
+  if (mth == MONOLIS_ITER_PIPECG && m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] != 0) {
+    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64 (MONOLIS_B200_PRECISION_FP64)\n");
     return false;
   }
   if (pc != MONOLIS_PREC_NONE && pc != MONOLIS_PREC_DIAG) {

@@ -149,10 +149,46 @@ __device__ void fin_bicg(SolverState* st, double rr, double rrt, double* hist) {
   st->iter += 1;
 }
 
+// PipeCG (src/iterative/PipeCG.f90:93-149). Convergence check of an
+// iteration (or the initial residual when iter == 0): rr = <R,R>.
+__device__ void fin_pipe_check(SolverState* st, double rr, double* hist) {
+  if (st->iter == 0) {
+    st->B2 = rr;
+    if (rr == 0.0) { st->done = 1; st->status = kZeroRhs; return; }
+    st->rho = 1.0;    // gamma (PipeCG.f90:85)
+    st->alpha = 1.0;  // alpha (PipeCG.f90:86)
+    st->iter = 1;
+    return;
+  }
+  const double resid = sqrt(rr / st->B2);
+  record(st, hist, resid);
+  if (resid < st->tol) { st->done = 1; st->status = kOk; return; }
+  if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
+  if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
+  st->iter += 1;
+}
+
+// PipeCG scalars from gamma = <R,U>, delta = <V,U> (PipeCG.f90:100-113);
+// rho holds gamma, c2 delta.
+__device__ void fin_pipe_dots(SolverState* st, double g, double d) {
+  const double gamma1 = 1.0 / st->rho;
+  const double alpha1 = 1.0 / st->alpha;
+  st->rho = g;
+  st->c2 = d;
+  if (1 < st->iter) {
+    st->beta = g * gamma1;
+    st->alpha = g / (d - st->beta * g * alpha1);
+  } else {
+    st->alpha = g / d;
+    st->beta = 0.0;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // FP64 residual kernel: r = b - A x, then z = M^-1 r (CG) and the two dots.
 // mode 0: CG (dots <r,r>, <r,z>); mode 1: BiCGSTAB (dots <r,r>, <r,rt>;
-// at iter 0 also rt = r). Runs for the initial residual and, on iterations
+// at iter 0 also rt = r); mode 2: PipeCG (z is U = M^-1 r; <r,r> decides
+// convergence). Runs for the initial residual and, on iterations
 // with iter % iter_RR == 0, after the update kernel has raised rr_flag.
 // ---------------------------------------------------------------------------
 template <int B, int U, class V, class T>
@@ -175,7 +211,7 @@ __global__ void __launch_bounds__(kThreads)
       r[i] = t[c];
       v[0] += (double)t[c] * (double)t[c];
     }
-    if (mode == 0) {
+    if (mode != 1) {  // CG and PipeCG: z (PipeCG: U) = M^-1 r
       T w[B];
 #pragma unroll
       for (int c = 0; c < B; c++) w[c] = t[c];
@@ -203,6 +239,7 @@ __global__ void __launch_bounds__(kThreads)
     }
     st->rr_flag = 0;
     if (mode == 0) fin_cg(st, tot[0], tot[1], hist);
+    else if (mode == 2) fin_pipe_check(st, tot[0], hist);
     else fin_bicg(st, tot[0], tot[1], hist);
   });
 }
@@ -378,6 +415,92 @@ __global__ void shard_resid_kernel(SolverState* st, double* hist, int mode) {
   st->rr_flag = 0;
   if (mode == 0) fin_cg(st, st->red[0], st->red[1], hist);
   else fin_bicg(st, st->red[0], st->red[1], hist);
+}
+
+// ---------------------------------------------------------------------------
+// PipeCG kernels (src/iterative/PipeCG.f90:87-149). One iteration: the two
+// dots and M = M^-1 V in one pass, L = A M, then every vector update with
+// <R,R> in one pass; the replacement iteration (iter % iter_RR == 0)
+// recomputes R = B - A X, U = M^-1 R and V = A U instead of the R, U, V
+// recurrences.
+// ---------------------------------------------------------------------------
+// gamma = <R,U>, delta = <V,U>; M = M^-1 V
+template <int B, class T>
+__global__ void __launch_bounds__(kThreads)
+    pipe_dots_kernel(int N, const T* __restrict__ r, const T* __restrict__ u, const T* __restrict__ vv,
+                     T* __restrict__ mm, const T* __restrict__ alu, int prec, double* partials, unsigned int* ticket,
+                     SolverState* st) {
+  if (st->done) return;
+  double v[2] = {0.0, 0.0};
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) {
+    T w[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = (long long)row * B + c;
+      const T uv = u[i];
+      w[c] = vv[i];
+      v[0] += (double)r[i] * (double)uv;
+      v[1] += (double)w[c] * (double)uv;
+    }
+    if (prec) diag_row<B, T>(alu, N, row, w);
+#pragma unroll
+    for (int c = 0; c < B; c++) mm[(long long)row * B + c] = w[c];
+  }
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_pipe_dots(st, tot[0], tot[1]); });
+}
+
+// out = A in (no dot)
+template <int B, int U, class V, class T>
+__global__ void __launch_bounds__(kThreads)
+    pipe_spmv_kernel(SellView<V> A, const T* __restrict__ in, T* __restrict__ out, const SolverState* st) {
+  if (st->done) return;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+    T y[B];
+    sell_row<B, U, V, T>(A, in, row, y);
+#pragma unroll
+    for (int c = 0; c < B; c++) out[(long long)row * B + c] = y[c];
+  }
+}
+
+// Z = beta Z + L, Q = beta Q + M, S = beta S + V, P = beta P + U; then
+// R -= alpha S, U -= alpha Q, V -= alpha Z, X += alpha P and <R,R>, or on a
+// replacement iteration X += alpha P only (the residual kernel follows).
+// Each update is the reference's AXPBY with a unit second factor: two
+// roundings.
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    pipe_update_kernel(long long n, T* __restrict__ x, T* __restrict__ r, T* __restrict__ u, T* __restrict__ vv,
+                       T* __restrict__ q, T* __restrict__ p, T* __restrict__ z, const T* __restrict__ l,
+                       const T* __restrict__ mm, T* __restrict__ s, double* partials, unsigned int* ticket,
+                       SolverState* st, double* hist) {
+  if (st->done) return;
+  const bool rr_iter = (st->iter % st->iter_rr) == 0;
+  const T alpha = (T)st->alpha, beta = (T)st->beta;
+  double v[1] = {0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const T zi = add_rn(mul_rn(beta, z[i]), l[i]);
+    const T qi = add_rn(mul_rn(beta, q[i]), mm[i]);
+    const T vi = vv[i];
+    const T si = add_rn(mul_rn(beta, s[i]), vi);
+    const T pi = add_rn(mul_rn(beta, p[i]), u[i]);
+    z[i] = zi;
+    q[i] = qi;
+    s[i] = si;
+    p[i] = pi;
+    if (!rr_iter) {
+      const T ri = add_rn(mul_rn(-alpha, si), r[i]);
+      r[i] = ri;
+      u[i] = add_rn(mul_rn(-alpha, qi), u[i]);
+      vv[i] = add_rn(mul_rn(-alpha, zi), vi);
+      v[0] += (double)ri * (double)ri;
+    }
+    x[i] = add_rn(mul_rn(alpha, pi), x[i]);
+  }
+  if (rr_iter) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
+    return;
+  }
+  grid_reduce<1>(v, partials, ticket, [&](double* tot) { fin_pipe_check(st, tot[0], hist); });
 }
 
 // ---------------------------------------------------------------------------
@@ -1058,7 +1181,11 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const long long n = (long long)N * nd;
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
-  if (p.method != 1 && p.method != 5) return kBadInput;
+  if (p.method != 1 && p.method != 3 && p.method != 5) return kBadInput;
+  if (p.method == 3 && (p.precision != 0 || p.shard)) {
+    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64 on one rank\n");
+    return kBadInput;
+  }
   if (p.shard && (p.precision != 0 || p.np_rows < N)) {
     fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG or BiCGSTAB\n");
     return kBadInput;
@@ -1072,7 +1199,9 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     if (rc) return rc;
   }
 
-  const int iter_rr = p.iter_rr > 0 ? p.iter_rr : 200;
+  // true-residual interval: 200 for CG and BiCGSTAB, 50 for PipeCG (CG.f90:40,
+  // BiCGSTAB.f90:41, PipeCG.f90:43)
+  const int iter_rr = p.iter_rr > 0 ? p.iter_rr : (p.method == 3 ? 50 : 200);
   // Iterations per graph launch. FP64: the replacement iterations must fall
   // on the last iteration of a batch, so the batch divides iter_RR.
   int batch, period;
@@ -1168,6 +1297,39 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           }
           if (ev) cudaEventRecord(ev[5], ss);
         };
+      } else if (p.method == 3) {
+        // PipeCG: R, U, V, Q, P, Z, L, M, S (PipeCG.f90:51-59)
+        double *r = vec.get<double>(n), *u = vec.get<double>(n), *vv = vec.get<double>(n), *q = vec.get<double>(n),
+               *pp = vec.get<double>(n), *z = vec.get<double>(n), *l = vec.get<double>(n), *mm = vec.get<double>(n),
+               *sv = vec.get<double>(n);
+        if (!r || !u || !vv || !q || !pp || !z || !l || !mm || !sv) return kCudaError;
+        for (double* w : {q, pp, z, sv})  // monolis_alloc_R_1d zero-fills
+          if (cudaMemsetAsync(w, 0, sizeof(double) * n, s) != cudaSuccess) return kCudaError;
+        auto k_dots = pipe_dots_kernel<B, double>;
+        auto k_mv = pipe_spmv_kernel<B, U, double, double>;
+        auto k_upd = pipe_update_kernel<double>;
+        const int g_dots = pgrid(k_dots), g_mv = pgrid(k_mv), g_upd = pgrid(k_upd);
+        // R = B - A X, U = M^-1 R, B2 (PipeCG.f90:67-83); V = A U
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st, hist);
+        k_mv<<<g_mv, kThreads, 0, s>>>(A64, u, vv, st);
+        plan.kernels = 5;
+        plan.kind = {1, 0, 1, 0, 0};
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          k_dots<<<g_dots, kThreads, 0, ss>>>(N, r, u, vv, mm, alu, prec, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          k_mv<<<g_mv, kThreads, 0, ss>>>(A64, mm, l, st);
+          if (ev) cudaEventRecord(ev[2], ss);
+          k_upd<<<g_upd, kThreads, 0, ss>>>(n, x, r, u, vv, q, pp, z, l, mm, sv, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[3], ss);
+          if (special)
+            k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[4], ss);
+          if (special) k_mv<<<g_mv, kThreads, 0, ss>>>(A64, u, vv, st);
+          if (ev) cudaEventRecord(ev[5], ss);
+        };
+        plan.launches = 3;
+        plan.launches_special = 5;
       } else if (p.method == 1) {
         double *r = vec.get<double>(n), *z = vec.get<double>(n), *q = vec.get<double>(n), *pp = vec.get<double>(n);
         if (!r || !z || !q || !pp) return kCudaError;

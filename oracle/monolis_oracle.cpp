@@ -41,9 +41,11 @@
 
 namespace {
 
-// iter_RR of src/iterative/CG.f90:40 and BiCGSTAB.f90:41 (200); settable
-// through oracle_set_iter_rr() so tests can cross several replacements.
+// iter_RR of src/iterative/CG.f90:40 and BiCGSTAB.f90:41 (200) and of
+// src/iterative/PipeCG.f90:43 (50); settable through oracle_set_iter_rr() so
+// tests can cross several replacements.
 int g_iter_rr = 200;
+int g_iter_rr_pipe = 50;
 
 double now_sec() {
   using namespace std::chrono;
@@ -502,6 +504,78 @@ int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t)
   return status ? status : 1;
 }
 
+// src/iterative/PipeCG.f90:18-160 (pipelined CG: one reduction phase per
+// iteration whose sums are independent of the product that follows)
+int solver_PipeCG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
+  double* X = a->R.X;
+  const double* B = a->R.B;
+  const int iter_RR = g_iter_rr_pipe;
+  long long nndof = (long long)a->N * a->NDOF;
+  if (prm->Iarray[MONOLIS_PRM_I_IS_INIT_X] == MONOLIS_I_TRUE)
+    for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
+  std::vector<double> R(nndof), U(nndof), V(nndof), Q(nndof), P(nndof), Z(nndof), L(nndof), M(nndof), S(nndof);
+  residual(a, X, B, R.data(), nndof, t);
+  double B2 = dot(nndof, R.data(), R.data());
+  if (B2 == 0.0) {  // src/linalg/mat_converge.f90:40-48
+    fprintf(stderr, "** monolis error: norm of RHS vector B is 0.0\n");
+    for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
+    return 0;
+  }
+  double t1 = now_sec();
+  precond_apply(a, pc, nndof, R.data(), U.data());
+  t.prec += now_sec() - t1;
+  t1 = now_sec();
+  matvec(a, a->N, U.data(), V.data());
+  t.spmv += now_sec() - t1;
+  double gamma = 1.0, alpha = 1.0, beta, delta;
+  int status = 0;
+  for (int iter = 1; iter <= prm->Iarray[MONOLIS_PRM_I_MAX_ITER]; iter++) {
+    t1 = now_sec();
+    const double cg1 = dot(nndof, R.data(), U.data());  // PipeCG.f90:88-91 (<R,R> there is not used)
+    const double cg2 = dot(nndof, V.data(), U.data());
+    t.dotp += now_sec() - t1;
+    t1 = now_sec();
+    precond_apply(a, pc, nndof, V.data(), M.data());
+    t.prec += now_sec() - t1;
+    t1 = now_sec();
+    matvec(a, a->N, M.data(), L.data());
+    t.spmv += now_sec() - t1;
+    const double gamma1 = 1.0 / gamma;
+    const double alpha1 = 1.0 / alpha;
+    gamma = cg1;
+    delta = cg2;
+    if (1 < iter) {
+      beta = gamma * gamma1;
+      alpha = gamma / (delta - beta * gamma * alpha1);
+    } else {
+      alpha = gamma / delta;
+      beta = 0.0;
+    }
+    axpby(nndof, beta, Z.data(), 1.0, L.data(), Z.data());
+    axpby(nndof, beta, Q.data(), 1.0, M.data(), Q.data());
+    axpby(nndof, beta, S.data(), 1.0, V.data(), S.data());
+    axpby(nndof, beta, P.data(), 1.0, U.data(), P.data());
+    if (iter % iter_RR == 0) {
+      axpby(nndof, alpha, P.data(), 1.0, X, X);
+      residual(a, X, B, R.data(), nndof, t);
+      t1 = now_sec();
+      precond_apply(a, pc, nndof, R.data(), U.data());
+      t.prec += now_sec() - t1;
+      t1 = now_sec();
+      matvec(a, a->N, U.data(), V.data());
+      t.spmv += now_sec() - t1;
+    } else {
+      axpby(nndof, -alpha, S.data(), 1.0, R.data(), R.data());
+      axpby(nndof, -alpha, Q.data(), 1.0, U.data(), U.data());
+      axpby(nndof, -alpha, Z.data(), 1.0, V.data(), V.data());
+      axpby(nndof, alpha, P.data(), 1.0, X, X);
+    }
+    if (check_converge(prm, nndof, R.data(), B2, iter, t, &status)) return 0;
+    if (status == 3) return 3;
+  }
+  return status ? status : 1;
+}
+
 const char* str_iter(int m) {
   static const char* names[] = {"CG", "GropCG", "PipeCG", "PipeCR", "BiCGSTAB", "PipeBiCGSTAB",
                                 "BiCGSTAB_noprec", "PipeBiCGSTAB_noprec", "BiCGSTAB_N128", "SOR",
@@ -535,6 +609,7 @@ void solve_main(MONOLIS_PRM* prm, MONOLIS_MAT* a) {
   int status;
   if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_CG) status = solver_CG(prm, a, pc, t);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_BICGSTAB) status = solver_BiCGSTAB(prm, a, pc, t);
+  else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_PIPECG) status = solver_PipeCG(prm, a, pc, t);
   else error_stop("please select a linear solver for real numbers");
   I[MONOLIS_PRM_I_IERR] = status;
   Rr[MONOLIS_R_TIME_SPMV] = t.spmv;
@@ -830,7 +905,10 @@ void oracle_set_threads(int n) {
   (void)n;
 #endif
 }
-void oracle_set_iter_rr(int n) { g_iter_rr = n > 0 ? n : 200; }
+void oracle_set_iter_rr(int n) {
+  g_iter_rr = n > 0 ? n : 200;
+  g_iter_rr_pipe = n > 0 ? n : 50;
+}
 
 int oracle_get_threads(void) {
 #ifdef _OPENMP

@@ -166,6 +166,9 @@ def test_inner_product(gpu, oracle):
     ("convection_diffusion", dict(n=24, peclet=5.0), api.ITER_BICGSTAB),
     ("convection_diffusion", dict(n=24, peclet=50.0), api.ITER_BICGSTAB),
     ("laplacian", dict(n=16), api.ITER_BICGSTAB),
+    ("laplacian", dict(n=32), api.ITER_PIPECG),      # PipeCG: iter_RR 50, crossed
+    ("elasticity", dict(n=12), api.ITER_PIPECG),
+    ("diffusion_kappa", dict(n=12), api.ITER_PIPECG),
 ])
 @pytest.mark.parametrize("prec", [api.PREC_DIAG, api.PREC_NONE])
 def test_solver_parity_fp64(gpu, oracle, problem, kw, method, prec):
@@ -200,6 +203,8 @@ def test_cg_parity_past_residual_replacement(gpu, oracle):
     ("convection_diffusion", dict(n=40, peclet=50.0), api.ITER_BICGSTAB, api.PREC_DIAG, 15),
     ("diffusion_kappa", dict(n=24), api.ITER_CG, api.PREC_DIAG, 25),
     ("elasticity", dict(n=16), api.ITER_CG, api.PREC_NONE, 30),
+    ("elasticity", dict(n=12), api.ITER_PIPECG, api.PREC_DIAG, 20),
+    ("laplacian", dict(n=24), api.ITER_PIPECG, api.PREC_NONE, 15),
 ])
 def test_parity_with_frequent_residual_replacement(gpu, oracle, problem, kw, method, prec, rr):
     """The replacement interval (200 in the reference) shortened in both
@@ -211,7 +216,7 @@ def test_parity_with_frequent_residual_replacement(gpu, oracle, problem, kw, met
     try:
         xo, it_o, _, st_o = solve(mo, b, method, prec)
     finally:
-        oracle.oracle_set_iter_rr(200)
+        oracle.oracle_set_iter_rr(0)  # back to the reference intervals (200; PipeCG 50)
     xp, it_p, _, st_p = solve(mp, b, method, prec)
     assert it_o > 2 * rr and st_o == 0 and st_p == 0
     assert abs(it_p - it_o) <= 2, (it_p, it_o)

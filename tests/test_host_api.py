@@ -145,8 +145,12 @@ def test_unsupported_method_reports_status(product):
     elem = np.array([[0, 1]], dtype=np.int32)
     m.get_nonzero_pattern_by_simple_mesh(2, 2, 1, elem)
     m.quiet()
-    m.set_method(3)  # PipeCG: not provided
+    m.set_method(2)  # GropCG: not provided
     x = np.zeros(2)
+    m.solve(np.ones(2), x)
+    assert m.get_error_tag() == 5 and np.all(x == 0.0)
+    m.set_method(api.ITER_PIPECG)  # provided in FP64 only
+    m.set_precision(1)
     m.solve(np.ones(2), x)
     assert m.get_error_tag() == 5 and np.all(x == 0.0)
 
