@@ -916,9 +916,10 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   }
   const bool sharded = ncomm != nullptr;
   if (sharded && (transpose ||
-                  (I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_CG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_BICGSTAB) ||
+                  (I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_CG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_BICGSTAB &&
+                   I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_PIPECG) ||
                   I[MONOLIS_B200_PRM_I_PRECISION] != 0)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG or BiCGSTAB\n");
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG, PipeCG or BiCGSTAB\n");
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
     return MONOLIS_B200_BAD_INPUT;
   }

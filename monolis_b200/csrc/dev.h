@@ -174,6 +174,10 @@ int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s);
 // shard_halo_join makes s wait for it
 int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s);
 int shard_halo_join(const ShardPlan& sp, cudaStream_t s);
+// all-reduce of k doubles on the side stream, after the work already on s
+// (shard_halo_join makes s wait for it); no other collective is issued until
+// it has been joined
+int shard_allreduce_fork(const ShardPlan& sp, double* d, int k, cudaStream_t s);
 int shard_allreduce(const ShardPlan& sp, double* d, int k, cudaStream_t s);
 
 struct SolveParams {

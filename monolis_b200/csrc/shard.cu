@@ -278,6 +278,14 @@ int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s) {
   return rc;
 }
 
+int shard_allreduce_fork(const ShardPlan& sp, double* d, int k, cudaStream_t s) {
+  MB_CUDA_OK(cudaEventRecord(sp.ev_fork, s));
+  MB_CUDA_OK(cudaStreamWaitEvent(sp.side, sp.ev_fork, 0));
+  const int rc = shard_allreduce(sp, d, k, sp.side);
+  MB_CUDA_OK(cudaEventRecord(sp.ev_join, sp.side));
+  return rc;
+}
+
 int shard_halo_join(const ShardPlan& sp, cudaStream_t s) {
   MB_CUDA_OK(cudaStreamWaitEvent(s, sp.ev_join, 0));
   return kOk;

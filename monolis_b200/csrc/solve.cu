@@ -414,6 +414,7 @@ __global__ void shard_resid_kernel(SolverState* st, double* hist, int mode) {
   if (st->done || !(st->iter == 0 || st->rr_flag)) return;
   st->rr_flag = 0;
   if (mode == 0) fin_cg(st, st->red[0], st->red[1], hist);
+  else if (mode == 2) fin_pipe_check(st, st->red[0], hist);
   else fin_bicg(st, st->red[0], st->red[1], hist);
 }
 
@@ -446,7 +447,14 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int c = 0; c < B; c++) mm[(long long)row * B + c] = w[c];
   }
-  grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_pipe_dots(st, tot[0], tot[1]); });
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // the scalars after the all-reduce (shard_pipe_dots_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
+    fin_pipe_dots(st, tot[0], tot[1]);
+  });
 }
 
 // out = A in (no dot)
@@ -500,7 +508,23 @@ __global__ void __launch_bounds__(kThreads)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->rr_flag = 1;
     return;
   }
-  grid_reduce<1>(v, partials, ticket, [&](double* tot) { fin_pipe_check(st, tot[0], hist); });
+  grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // the check after the all-reduce (shard_pipe_check_kernel)
+      st->red[0] = tot[0];
+      return;
+    }
+    fin_pipe_check(st, tot[0], hist);
+  });
+}
+
+// Multi-rank PipeCG: the scalar steps with the all-reduced sums in red[].
+__global__ void shard_pipe_dots_kernel(SolverState* st) {
+  if (st->done) return;
+  fin_pipe_dots(st, st->red[0], st->red[1]);
+}
+__global__ void shard_pipe_check_kernel(SolverState* st, double* hist) {
+  if (st->done || (st->iter % st->iter_rr) == 0) return;
+  fin_pipe_check(st, st->red[0], hist);
 }
 
 // ---------------------------------------------------------------------------
@@ -1182,12 +1206,12 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
   if (p.method != 1 && p.method != 3 && p.method != 5) return kBadInput;
-  if (p.method == 3 && (p.precision != 0 || p.shard)) {
-    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64 on one rank\n");
+  if (p.method == 3 && p.precision != 0) {
+    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64\n");
     return kBadInput;
   }
   if (p.shard && (p.precision != 0 || p.np_rows < N)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG or BiCGSTAB\n");
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG, PipeCG or BiCGSTAB\n");
     return kBadInput;
   }
   // vectors gathered by the SpMV hold the ghost rows too
@@ -1294,6 +1318,65 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
             k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
             shard_allreduce(*sp, st->red, 2, ss);
             shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist, 0);
+          }
+          if (ev) cudaEventRecord(ev[5], ss);
+        };
+      } else if (p.method == 3 && p.shard) {
+        // multi-rank PipeCG: the all-reduce of <R,U>, <V,U> runs on the side
+        // stream while this rank multiplies L = A M (PipeCG.f90:88-95: the
+        // sums do not feed the product)
+        const ShardPlan* sp = p.shard;
+        double *r = vec.get<double>(n), *u = vec.get<double>(n_ext), *vv = vec.get<double>(n),
+               *q = vec.get<double>(n), *pp = vec.get<double>(n), *z = vec.get<double>(n), *l = vec.get<double>(n),
+               *mm = vec.get<double>(n_ext), *sv = vec.get<double>(n);
+        if (!r || !u || !vv || !q || !pp || !z || !l || !mm || !sv) return kCudaError;
+        for (double* w : {q, pp, z, sv})
+          if (cudaMemsetAsync(w, 0, sizeof(double) * n, s) != cudaSuccess) return kCudaError;
+        for (double* w : {u, mm})
+          if (cudaMemsetAsync(w, 0, sizeof(double) * n_ext, s) != cudaSuccess) return kCudaError;
+        auto k_dots = pipe_dots_kernel<B, double>;
+        auto k_mv = pipe_spmv_kernel<B, U, double, double>;
+        auto k_upd = pipe_update_kernel<double>;
+        const int g_dots = pgrid(k_dots), g_mv = pgrid(k_mv), g_upd = pgrid(k_upd);
+        int rc2 = shard_halo(*sp, x, s);
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st, hist);
+        if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+        shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 2);
+        if (!rc2) rc2 = shard_halo(*sp, u, s);
+        k_mv<<<g_mv, kThreads, 0, s>>>(A64, u, vv, st);
+        if (rc2) return rc2;
+        const int hk = (sp->n_send > 0) + (sp->n_recv > 0);
+        plan.kernels = 5;
+        plan.kind = {1, 0, 1, 0, 0};
+        plan.launches = 5 + hk;
+        plan.launches_special = 7 + 3 * hk;
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool special) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          k_dots<<<g_dots, kThreads, 0, ss>>>(N, r, u, vv, mm, alu, prec, partials, ticket, st);
+          if (ev) cudaEventRecord(ev[1], ss);
+          shard_halo(*sp, mm, ss);
+          shard_allreduce_fork(*sp, st->red, 2, ss);  // in flight during the product
+          k_mv<<<g_mv, kThreads, 0, ss>>>(A64, mm, l, st);
+          shard_halo_join(*sp, ss);
+          shard_pipe_dots_kernel<<<1, 1, 0, ss>>>(st);
+          if (ev) cudaEventRecord(ev[2], ss);
+          k_upd<<<g_upd, kThreads, 0, ss>>>(n, x, r, u, vv, q, pp, z, l, mm, sv, partials, ticket, st, hist);
+          if (!special) {
+            shard_allreduce(*sp, st->red, 1, ss);
+            shard_pipe_check_kernel<<<1, 1, 0, ss>>>(st, hist);
+          }
+          if (ev) cudaEventRecord(ev[3], ss);
+          if (special) {
+            shard_halo(*sp, x, ss);
+            k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st,
+                                                 hist);
+            shard_allreduce(*sp, st->red, 2, ss);
+            shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist, 2);
+          }
+          if (ev) cudaEventRecord(ev[4], ss);
+          if (special) {
+            shard_halo(*sp, u, ss);
+            k_mv<<<g_mv, kThreads, 0, ss>>>(A64, u, vv, st);
           }
           if (ev) cudaEventRecord(ev[5], ss);
         };

@@ -98,6 +98,10 @@ def _worker(rank, world, port, problem, q, method="cg"):
             it = _bicgstab(r, x, p, nd, n, npr, halo, gdot, prec)
             q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
             return
+        if method == "pipecg":
+            it = _pipecg(r, x, bl, p, nd, n, npr, halo, gdot, prec)
+            q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
+            return
         z = prec(r)
         B2 = gdot(bl, bl)
         rho = gdot(r, z)
@@ -156,6 +160,73 @@ def _bicgstab(r, x, p, nd, n, npr, halo, gdot, prec):
             return it
         rho1, rho = rho, gdot(r, rt)
     return 5000
+
+
+def _pipecg(r, x, bl, p, nd, n, npr, halo, gdot, prec, iter_rr=50):
+    """PipeCG of the device code's multi-rank plan (src/iterative/PipeCG.f90:67-149):
+    U and M get their ghost entries before their products; <R,U> and <V,U>
+    are all-reduced together (on the device, while L = A M runs), <R,R> for
+    the convergence check. Returns the iteration count."""
+    B2 = gdot(r, r)
+    u = np.zeros(npr * nd)
+    u[:n * nd] = prec(r)
+    halo(u)
+    v = local_matvec(p, nd, u)
+    m = np.zeros(npr * nd)
+    z, qv, s, pv = (np.zeros(n * nd) for _ in range(4))
+    gamma, alpha = 1.0, 1.0
+    for it in range(1, 5000):
+        g, d = gdot(r, u), gdot(v, u)
+        m[:n * nd] = prec(v)
+        halo(m)
+        l = local_matvec(p, nd, m)
+        gamma1, alpha1 = 1.0 / gamma, 1.0 / alpha
+        gamma, delta = g, d
+        if it > 1:
+            beta = gamma * gamma1
+            alpha = gamma / (delta - beta * gamma * alpha1)
+        else:
+            alpha, beta = gamma / delta, 0.0
+        z = beta * z + l
+        qv = beta * qv + m[:n * nd]
+        s = beta * s + v
+        pv = beta * pv + u[:n * nd]
+        if it % iter_rr == 0:
+            x[:n * nd] += alpha * pv
+            halo(x)
+            r = bl[:n * nd] - local_matvec(p, nd, x)
+            u[:n * nd] = prec(r)
+            halo(u)
+            v = local_matvec(p, nd, u)
+        else:
+            r = r - alpha * s
+            u[:n * nd] = u[:n * nd] - alpha * qv
+            v = v - alpha * z
+            x[:n * nd] += alpha * pv
+        if np.sqrt(gdot(r, r) / B2) < 1e-8:
+            return it
+    return 5000
+
+
+@pytest.mark.parametrize("problem,world", [("laplacian", 2), ("elasticity", 3)])
+def test_partitioned_pipecg_matches_single_rank(problem, world, oracle):
+    from monolis_b200 import api
+    from helpers import solve
+    m, b = global_system(problem)
+    nd = m.NDOF
+    x_ref, it_ref, _, st = solve(m, b, api.ITER_PIPECG, api.PREC_DIAG, tol=1e-8)
+    assert st == 0
+    out = _run_ranks(problem, world, "pipecg", 33900 + (os.getpid() % 2000) + 13 * world)
+    x = np.zeros_like(b)
+    its = set()
+    for rank, glob, xl, it in out:
+        glob = np.array(glob)
+        x[(glob[:, None] * nd + np.arange(nd)).reshape(-1)] = xl
+        its.add(it)
+    assert len(its) == 1
+    assert abs(its.pop() - it_ref) <= 2
+    x_tight, _, _, _ = solve(m, b, api.ITER_PIPECG, api.PREC_DIAG, tol=1e-12)
+    assert np.linalg.norm(x - x_tight) / np.linalg.norm(x_tight) < 1e-6
 
 
 def _run_ranks(problem, world, method, port):

@@ -1,6 +1,6 @@
 """The multi-rank device path (halo updates through NCCL, dot products summed
 by an NCCL all-reduce, scalar updates in separate one-thread kernels), FP64
-CG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
+CG, PipeCG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
 bits and iteration count of the single-rank solve, also past the
 true-residual replacement at iteration 200. (Runs here have one GPU; more
 ranks cannot share it.)"""
@@ -22,6 +22,8 @@ pytestmark = pytest.mark.gpu
     ("convection_diffusion", dict(n=16, peclet=0.5), api.ITER_BICGSTAB, 7),
     ("laplacian", dict(n=24), api.ITER_BICGSTAB, 5),
     ("elasticity", dict(n=10), api.ITER_BICGSTAB, 0),
+    ("elasticity", dict(n=12), api.ITER_PIPECG, 0),
+    ("laplacian", dict(n=20), api.ITER_PIPECG, 9),
 ])
 def test_sharded_path_one_rank_bit_identical(gpu, problem, kw, method, rr):
     """rr > 0: true residual every rr iterations (instead of 200), so the
@@ -69,6 +71,7 @@ def test_sharded_path_rejects_unsupported(gpu):
     ("laplacian", dict(n=14), api.ITER_CG),
     ("elasticity", dict(n=7), api.ITER_CG),
     ("convection_diffusion", dict(n=14, peclet=5.0), api.ITER_BICGSTAB),
+    ("laplacian", dict(n=14), api.ITER_PIPECG),
 ])
 def test_sharded_boundary_rows_through_self_halo(gpu, problem, kw, method):
     """A one-rank system whose rows read some columns through ghost entries:
