@@ -242,7 +242,7 @@ int monolis_b200_device_solve_multi_R(MONOLIS* mat, int n_rhs, const double* d_B
  * ids). Attaching an NCCL communicator to a MONOLIS_COM makes
  * monolis_solve_R(mat, com, b, x) solve the distributed system on the GPUs:
  * halo updates before every product, dot products summed over the ranks
- * (FP64 CG, PipeCG or BiCGSTAB; b and x hold NP*ndof entries). Rank 0 creates the id, every rank
+ * (FP64 CG, GropCG, PipeCG or BiCGSTAB; b and x hold NP*ndof entries). Rank 0 creates the id, every rank
  * receives it (by any means, e.g. MPI or torch.distributed) and calls
  * monolis_b200_com_init_nccl with its current CUDA device set. NCCL is
  * loaded at run time (libnccl.so.2). No counterpart in the reference (which

@@ -20,6 +20,7 @@ PRODUCT_SO = os.path.join(_HERE, "libmonolis_b200.so")
 
 # ---- constants (include/monolis.h, include/monolis_b200.h) ----
 ITER_CG = 1
+ITER_GROPCG = 2
 ITER_PIPECG = 3
 ITER_BICGSTAB = 5
 PREC_NONE = 0

@@ -536,13 +536,15 @@ void print_summary(MONOLIS* m) {
 bool method_supported(const MONOLIS* m) {
   const int mth = m->prm.Iarray[MONOLIS_PRM_I_METHOD];
   const int pc = m->prm.Iarray[MONOLIS_PRM_I_PRECOND];
-  if (mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG) {
-    fprintf(stderr, "** monolis_b200: solver %s is not provided by this library (CG, PipeCG, BiCGSTAB)\n",
+  if (mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG &&
+      mth != MONOLIS_ITER_GROPCG) {
+    fprintf(stderr,
+            "** monolis_b200: solver %s is not provided by this library (CG, GropCG, PipeCG, BiCGSTAB)\n",
             str_iter(mth));
     return false;
   }
-  if (mth == MONOLIS_ITER_PIPECG && m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] != 0) {
-    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64 (MONOLIS_B200_PRECISION_FP64)\n");
+  if ((mth == MONOLIS_ITER_PIPECG || mth == MONOLIS_ITER_GROPCG) && m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] != 0) {
+    fprintf(stderr, "** monolis_b200: %s runs in FP64 (MONOLIS_B200_PRECISION_FP64)\n", str_iter(mth));
     return false;
   }
   if (pc != MONOLIS_PREC_NONE && pc != MONOLIS_PREC_DIAG) {
@@ -917,9 +919,9 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   const bool sharded = ncomm != nullptr;
   if (sharded && (transpose ||
                   (I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_CG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_BICGSTAB &&
-                   I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_PIPECG) ||
+                   I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_PIPECG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_GROPCG) ||
                   I[MONOLIS_B200_PRM_I_PRECISION] != 0)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG, PipeCG or BiCGSTAB\n");
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB)\n");
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
     return MONOLIS_B200_BAD_INPUT;
   }

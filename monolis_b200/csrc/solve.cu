@@ -184,6 +184,24 @@ __device__ void fin_pipe_dots(SolverState* st, double g, double d) {
   }
 }
 
+// GropCG (src/iterative/GropCG.f90:88-125); rho holds gamma, c2 delta.
+__device__ void fin_grop_alpha(SolverState* st, double d) {
+  st->c2 = d;
+  st->alpha = st->rho / d;  // GropCG.f90:93
+}
+// gamma1 = <R,U>, rr = <R,R>: beta, gamma (GropCG.f90:111-112), then the
+// convergence check of the iteration
+__device__ void fin_grop(SolverState* st, double g1, double rr, double* hist) {
+  st->beta = g1 / st->rho;
+  st->rho = g1;
+  const double resid = sqrt(rr / st->B2);
+  record(st, hist, resid);
+  if (resid < st->tol) { st->done = 1; st->status = kOk; return; }
+  if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
+  if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
+  st->iter += 1;
+}
+
 // ---------------------------------------------------------------------------
 // FP64 residual kernel: r = b - A x, then z = M^-1 r (CG) and the two dots.
 // mode 0: CG (dots <r,r>, <r,z>); mode 1: BiCGSTAB (dots <r,r>, <r,rt>;
@@ -525,6 +543,106 @@ __global__ void shard_pipe_dots_kernel(SolverState* st) {
 __global__ void shard_pipe_check_kernel(SolverState* st, double* hist) {
   if (st->done || (st->iter % st->iter_rr) == 0) return;
   fin_pipe_check(st, st->red[0], hist);
+}
+
+// ---------------------------------------------------------------------------
+// GropCG kernels (src/iterative/GropCG.f90:88-125): delta = <P,S> with
+// Q = M^-1 S; the X, R, U updates with <R,U> and <R,R>; V = A U with the P and
+// S updates (one rank: fused; several: V stored while the sums of the
+// previous pass are all-reduced, then the P, S pass).
+// ---------------------------------------------------------------------------
+template <int B, class T>
+__global__ void __launch_bounds__(kThreads)
+    grop_q_kernel(int N, const T* __restrict__ p, const T* __restrict__ s, T* __restrict__ q,
+                  const T* __restrict__ alu, int prec, double* partials, unsigned int* ticket, SolverState* st) {
+  if (st->done) return;
+  double v[1] = {0.0};
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) {
+    T w[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = (long long)row * B + c;
+      w[c] = s[i];
+      v[0] += (double)p[i] * (double)w[c];
+    }
+    if (prec) diag_row<B, T>(alu, N, row, w);
+#pragma unroll
+    for (int c = 0; c < B; c++) q[(long long)row * B + c] = w[c];
+  }
+  grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {
+      st->red[0] = tot[0];
+      return;
+    }
+    fin_grop_alpha(st, tot[0]);
+  });
+}
+
+template <class T>
+__global__ void __launch_bounds__(kThreads)
+    grop_update_kernel(long long n, T* __restrict__ x, T* __restrict__ r, T* __restrict__ u,
+                       const T* __restrict__ p, const T* __restrict__ s, const T* __restrict__ q, double* partials,
+                       unsigned int* ticket, SolverState* st, double* hist) {
+  if (st->done) return;
+  const T alpha = (T)st->alpha;
+  double v[2] = {0.0, 0.0};
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    x[i] = add_rn(mul_rn(alpha, p[i]), x[i]);
+    const T ri = add_rn(mul_rn(-alpha, s[i]), r[i]);
+    const T ui = add_rn(mul_rn(-alpha, q[i]), u[i]);
+    r[i] = ri;
+    u[i] = ui;
+    v[0] += (double)ri * (double)ui;
+    v[1] += (double)ri * (double)ri;
+  }
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
+    fin_grop(st, tot[0], tot[1], hist);
+  });
+}
+
+// V = A U, P = beta P + U, S = beta S + V (one rank: V is not stored)
+template <int B, int U, class V, class T>
+__global__ void __launch_bounds__(kThreads)
+    grop_spmv_kernel(SellView<V> A, const T* __restrict__ u, T* __restrict__ p, T* __restrict__ s,
+                     const SolverState* st) {
+  if (st->done) return;
+  const T beta = (T)st->beta;
+  for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
+    T y[B];
+    sell_row<B, U, V, T>(A, u, row, y);
+#pragma unroll
+    for (int c = 0; c < B; c++) {
+      const long long i = (long long)row * B + c;
+      p[i] = add_rn(mul_rn(beta, p[i]), u[i]);
+      s[i] = add_rn(mul_rn(beta, s[i]), y[c]);
+    }
+  }
+}
+
+// P = beta P + U, S = beta S + V (several ranks, after the all-reduce)
+template <class T>
+__global__ void grop_ps_kernel(long long n, T* __restrict__ p, T* __restrict__ s, const T* __restrict__ u,
+                               const T* __restrict__ vv, const SolverState* st) {
+  if (st->done) return;
+  const T beta = (T)st->beta;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    p[i] = add_rn(mul_rn(beta, p[i]), u[i]);
+    s[i] = add_rn(mul_rn(beta, s[i]), vv[i]);
+  }
+}
+
+__global__ void shard_grop_alpha_kernel(SolverState* st) {
+  if (st->done) return;
+  fin_grop_alpha(st, st->red[0]);
+}
+__global__ void shard_grop_kernel(SolverState* st, double* hist) {
+  if (st->done) return;
+  fin_grop(st, st->red[0], st->red[1], hist);
 }
 
 // ---------------------------------------------------------------------------
@@ -1205,13 +1323,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   const long long n = (long long)N * nd;
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
-  if (p.method != 1 && p.method != 3 && p.method != 5) return kBadInput;
-  if (p.method == 3 && p.precision != 0) {
-    fprintf(stderr, "** monolis_b200: PipeCG runs in FP64\n");
+  if (p.method != 1 && p.method != 2 && p.method != 3 && p.method != 5) return kBadInput;
+  if ((p.method == 2 || p.method == 3) && p.precision != 0) {
+    fprintf(stderr, "** monolis_b200: GropCG and PipeCG run in FP64\n");
     return kBadInput;
   }
   if (p.shard && (p.precision != 0 || p.np_rows < N)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 CG, PipeCG or BiCGSTAB\n");
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB)\n");
     return kBadInput;
   }
   // vectors gathered by the SpMV hold the ghost rows too
@@ -1232,6 +1350,9 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   if (p.precision == 1) {
     batch = p.batch > 0 ? p.batch : 16;
     period = 0;  // refreshes are decided on the device
+  } else if (p.method == 2) {
+    batch = p.batch > 0 ? p.batch : 25;
+    period = 0;  // GropCG.f90 runs no true-residual replacement
   } else {
     period = iter_rr;
     batch = p.batch > 0 && iter_rr % p.batch == 0 ? p.batch : largest_divisor_at_most(iter_rr, 25);
@@ -1320,6 +1441,58 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
             shard_resid_kernel<<<1, 1, 0, ss>>>(st, hist, 0);
           }
           if (ev) cudaEventRecord(ev[5], ss);
+        };
+      } else if (p.method == 2) {
+        // GropCG: R, U, V, Q, P, S (GropCG.f90:58-63); V only on several ranks
+        const ShardPlan* sp = p.shard;
+        double *r = vec.get<double>(n), *u = vec.get<double>(n_ext), *q = vec.get<double>(n),
+               *pp = vec.get<double>(n), *sv = vec.get<double>(n), *vv = sp ? vec.get<double>(n) : nullptr;
+        if (!r || !u || !q || !pp || !sv || (sp && !vv)) return kCudaError;
+        if (n_ext > n && cudaMemsetAsync(u, 0, sizeof(double) * n_ext, s) != cudaSuccess) return kCudaError;
+        auto k_q = grop_q_kernel<B, double>;
+        auto k_upd = grop_update_kernel<double>;
+        auto k_mvps = grop_spmv_kernel<B, U, double, double>;
+        auto k_mv = pipe_spmv_kernel<B, U, double, double>;
+        const int g_q = pgrid(k_q), g_upd = pgrid(k_upd), g_mvps = pgrid(k_mvps), g_mv = pgrid(k_mv);
+        // R = B - A X, U = M^-1 R, B2 and gamma = <R,U> (CG's initial step);
+        // P = U, S = A P (GropCG.f90:67-86)
+        int rc2 = sp ? shard_halo(*sp, x, s) : kOk;
+        k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, u, nullptr, alu, prec, 0, partials, ticket, st, hist);
+        if (sp) {
+          if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+          shard_resid_kernel<<<1, 1, 0, s>>>(st, hist, 0);
+          if (!rc2) rc2 = shard_halo(*sp, u, s);
+        }
+        if (cudaMemcpyAsync(pp, u, sizeof(double) * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return kCudaError;
+        k_mv<<<g_mv, kThreads, 0, s>>>(A64, u, sv, st);
+        if (rc2) return rc2;
+        const int hk = sp ? (sp->n_send > 0) + (sp->n_recv > 0) : 0;
+        plan.kernels = 3;
+        plan.kind = {2, 1, 0};
+        plan.launches = sp ? 6 + hk : 3;
+        plan.launches_special = plan.launches;
+        plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
+          if (ev) cudaEventRecord(ev[0], ss);
+          k_q<<<g_q, kThreads, 0, ss>>>(N, pp, sv, q, alu, prec, partials, ticket, st);
+          if (sp) {
+            shard_allreduce(*sp, st->red, 1, ss);
+            shard_grop_alpha_kernel<<<1, 1, 0, ss>>>(st);
+          }
+          if (ev) cudaEventRecord(ev[1], ss);
+          k_upd<<<g_upd, kThreads, 0, ss>>>(n, x, r, u, pp, sv, q, partials, ticket, st, hist);
+          if (ev) cudaEventRecord(ev[2], ss);
+          if (sp) {
+            // <R,U>, <R,R> all-reduced while V = A U runs (their sums do not feed the product)
+            shard_halo(*sp, u, ss);
+            shard_allreduce_fork(*sp, st->red, 2, ss);
+            k_mv<<<g_mv, kThreads, 0, ss>>>(A64, u, vv, st);
+            shard_halo_join(*sp, ss);
+            shard_grop_kernel<<<1, 1, 0, ss>>>(st, hist);
+            grop_ps_kernel<double><<<gvec, kThreads, 0, ss>>>(n, pp, sv, u, vv, st);
+          } else {
+            k_mvps<<<g_mvps, kThreads, 0, ss>>>(A64, u, pp, sv, st);
+          }
+          if (ev) cudaEventRecord(ev[3], ss);
         };
       } else if (p.method == 3 && p.shard) {
         // multi-rank PipeCG: the all-reduce of <R,U>, <V,U> runs on the side

@@ -576,6 +576,61 @@ int solver_PipeCG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
   return status ? status : 1;
 }
 
+// src/iterative/GropCG.f90:18-139 (Gropp's CG: <R,U> and <R,R> of an
+// iteration are independent of the product V = A U that follows; the
+// reference runs no true-residual replacement here)
+int solver_GropCG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
+  double* X = a->R.X;
+  const double* B = a->R.B;
+  long long nndof = (long long)a->N * a->NDOF;
+  if (prm->Iarray[MONOLIS_PRM_I_IS_INIT_X] == MONOLIS_I_TRUE)
+    for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
+  std::vector<double> R(nndof), U(nndof), V(nndof), Q(nndof), P(nndof), S(nndof);
+  residual(a, X, B, R.data(), nndof, t);
+  double B2 = dot(nndof, R.data(), R.data());
+  if (B2 == 0.0) {  // src/linalg/mat_converge.f90:40-48
+    fprintf(stderr, "** monolis error: norm of RHS vector B is 0.0\n");
+    for (long long i = 0; i < (long long)a->NP * a->NDOF; i++) X[i] = 0.0;
+    return 0;
+  }
+  double t1 = now_sec();
+  precond_apply(a, pc, nndof, R.data(), U.data());
+  t.prec += now_sec() - t1;
+  vcopy(nndof, U.data(), P.data());
+  t1 = now_sec();
+  matvec(a, a->N, P.data(), S.data());
+  t.spmv += now_sec() - t1;
+  t1 = now_sec();
+  double gamma = dot(nndof, R.data(), U.data());
+  t.dotp += now_sec() - t1;
+  int status = 0;
+  for (int iter = 1; iter <= prm->Iarray[MONOLIS_PRM_I_MAX_ITER]; iter++) {
+    t1 = now_sec();
+    const double delta = dot(nndof, P.data(), S.data());
+    t.dotp += now_sec() - t1;
+    t1 = now_sec();
+    precond_apply(a, pc, nndof, S.data(), Q.data());
+    t.prec += now_sec() - t1;
+    const double alpha = gamma / delta;
+    axpby(nndof, alpha, P.data(), 1.0, X, X);
+    axpby(nndof, -alpha, S.data(), 1.0, R.data(), R.data());
+    axpby(nndof, -alpha, Q.data(), 1.0, U.data(), U.data());
+    t1 = now_sec();
+    const double gamma1 = dot(nndof, R.data(), U.data());
+    t.dotp += now_sec() - t1;
+    t1 = now_sec();
+    matvec(a, a->N, U.data(), V.data());
+    t.spmv += now_sec() - t1;
+    const double beta = gamma1 / gamma;
+    gamma = gamma1;
+    axpby(nndof, beta, P.data(), 1.0, U.data(), P.data());
+    axpby(nndof, beta, S.data(), 1.0, V.data(), S.data());
+    if (check_converge(prm, nndof, R.data(), B2, iter, t, &status)) return 0;
+    if (status == 3) return 3;
+  }
+  return status ? status : 1;
+}
+
 const char* str_iter(int m) {
   static const char* names[] = {"CG", "GropCG", "PipeCG", "PipeCR", "BiCGSTAB", "PipeBiCGSTAB",
                                 "BiCGSTAB_noprec", "PipeBiCGSTAB_noprec", "BiCGSTAB_N128", "SOR",
@@ -610,6 +665,7 @@ void solve_main(MONOLIS_PRM* prm, MONOLIS_MAT* a) {
   if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_CG) status = solver_CG(prm, a, pc, t);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_BICGSTAB) status = solver_BiCGSTAB(prm, a, pc, t);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_PIPECG) status = solver_PipeCG(prm, a, pc, t);
+  else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_GROPCG) status = solver_GropCG(prm, a, pc, t);
   else error_stop("please select a linear solver for real numbers");
   I[MONOLIS_PRM_I_IERR] = status;
   Rr[MONOLIS_R_TIME_SPMV] = t.spmv;

@@ -98,6 +98,10 @@ def _worker(rank, world, port, problem, q, method="cg"):
             it = _bicgstab(r, x, p, nd, n, npr, halo, gdot, prec)
             q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
             return
+        if method == "gropcg":
+            it = _gropcg(r, x, p, nd, n, npr, halo, gdot, prec)
+            q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
+            return
         if method == "pipecg":
             it = _pipecg(r, x, bl, p, nd, n, npr, halo, gdot, prec)
             q.put((rank, p["glob"][:n].tolist(), x[:n * nd].tolist(), it))
@@ -208,15 +212,48 @@ def _pipecg(r, x, bl, p, nd, n, npr, halo, gdot, prec, iter_rr=50):
     return 5000
 
 
-@pytest.mark.parametrize("problem,world", [("laplacian", 2), ("elasticity", 3)])
-def test_partitioned_pipecg_matches_single_rank(problem, world, oracle):
+def _gropcg(r, x, p, nd, n, npr, halo, gdot, prec):
+    """GropCG of the device code's multi-rank plan (src/iterative/GropCG.f90:80-125):
+    U gets its ghost entries before V = A U, while <R,U> and <R,R> are
+    all-reduced; delta = <P,S> all-reduced before alpha. Returns the
+    iteration count."""
+    B2 = gdot(r, r)
+    u = np.zeros(npr * nd)
+    u[:n * nd] = prec(r)
+    pv = u[:n * nd].copy()
+    halo(u)
+    s = local_matvec(p, nd, u)
+    gamma = gdot(r, u)
+    for it in range(1, 5000):
+        delta = gdot(pv, s)
+        qv = prec(s)
+        alpha = gamma / delta
+        x[:n * nd] += alpha * pv
+        r = r - alpha * s
+        u[:n * nd] = u[:n * nd] - alpha * qv
+        gamma1, rr = gdot(r, u), gdot(r, r)
+        halo(u)
+        v = local_matvec(p, nd, u)
+        beta = gamma1 / gamma
+        gamma = gamma1
+        pv = beta * pv + u[:n * nd]
+        s = beta * s + v
+        if np.sqrt(rr / B2) < 1e-8:
+            return it
+    return 5000
+
+
+@pytest.mark.parametrize("problem,world,method", [("laplacian", 2, "pipecg"), ("elasticity", 3, "pipecg"),
+                                                  ("laplacian", 3, "gropcg"), ("elasticity", 2, "gropcg")])
+def test_partitioned_pipelined_cg_matches_single_rank(problem, world, method, oracle):
     from monolis_b200 import api
     from helpers import solve
+    mth = api.ITER_PIPECG if method == "pipecg" else api.ITER_GROPCG
     m, b = global_system(problem)
     nd = m.NDOF
-    x_ref, it_ref, _, st = solve(m, b, api.ITER_PIPECG, api.PREC_DIAG, tol=1e-8)
+    x_ref, it_ref, _, st = solve(m, b, mth, api.PREC_DIAG, tol=1e-8)
     assert st == 0
-    out = _run_ranks(problem, world, "pipecg", 33900 + (os.getpid() % 2000) + 13 * world)
+    out = _run_ranks(problem, world, method, 33900 + (os.getpid() % 2000) + 13 * world + (7 if method == "gropcg" else 0))
     x = np.zeros_like(b)
     its = set()
     for rank, glob, xl, it in out:
@@ -225,7 +262,7 @@ def test_partitioned_pipecg_matches_single_rank(problem, world, oracle):
         its.add(it)
     assert len(its) == 1
     assert abs(its.pop() - it_ref) <= 2
-    x_tight, _, _, _ = solve(m, b, api.ITER_PIPECG, api.PREC_DIAG, tol=1e-12)
+    x_tight, _, _, _ = solve(m, b, mth, api.PREC_DIAG, tol=1e-12)
     assert np.linalg.norm(x - x_tight) / np.linalg.norm(x_tight) < 1e-6
 
 

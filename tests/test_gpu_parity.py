@@ -169,15 +169,33 @@ def test_inner_product(gpu, oracle):
     ("laplacian", dict(n=32), api.ITER_PIPECG),      # PipeCG: iter_RR 50, crossed
     ("elasticity", dict(n=12), api.ITER_PIPECG),
     ("diffusion_kappa", dict(n=12), api.ITER_PIPECG),
+    ("laplacian", dict(n=32), api.ITER_GROPCG),
+    ("elasticity", dict(n=12), api.ITER_GROPCG),
+    ("diffusion_kappa", dict(n=12), api.ITER_GROPCG),
 ])
 @pytest.mark.parametrize("prec", [api.PREC_DIAG, api.PREC_NONE])
 def test_solver_parity_fp64(gpu, oracle, problem, kw, method, prec):
+    """Iterations within 2 of the oracle's. GropCG and PipeCG carry their
+    residuals by recurrence (GropCG never replaces them), which amplifies
+    the summation order of the dots: for them the bound is max(2, 3 x the
+    oracle's own spread over 1, 2, 4 and 8 threads)."""
     mp, b = build(gpu, problem, **kw)
     mo, _ = build(oracle, problem, **kw)
     xo, it_o, res_o, st_o = solve(mo, b, method, prec, tol=1e-8)
     xp, it_p, res_p, st_p = solve(mp, b, method, prec, tol=1e-8)
     assert st_o == 0 and st_p == 0, (st_o, st_p)
-    assert abs(it_p - it_o) <= 2, (it_p, it_o)
+    bound = 2
+    if method in (api.ITER_GROPCG, api.ITER_PIPECG):
+        its = [it_o]
+        try:
+            for th in (2, 4, 8):
+                oracle.oracle_set_threads(th)
+                mt, _ = build(oracle, problem, **kw)
+                its.append(solve(mt, b, method, prec, tol=1e-8)[1])
+        finally:
+            oracle.oracle_set_threads(1)
+        bound = max(2, 3 * (max(its) - min(its)))
+    assert abs(it_p - it_o) <= bound, (it_p, it_o, bound)
     assert res_p < 1e-8
     # both iterates satisfy the same tolerance; compare them at a tighter solve
     xo2, _, _, _ = solve(mo, b, method, prec, tol=1e-12)

@@ -1,6 +1,6 @@
 """The multi-rank device path (halo updates through NCCL, dot products summed
 by an NCCL all-reduce, scalar updates in separate one-thread kernels), FP64
-CG, PipeCG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
+CG, GropCG, PipeCG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
 bits and iteration count of the single-rank solve, also past the
 true-residual replacement at iteration 200. (Runs here have one GPU; more
 ranks cannot share it.)"""
@@ -24,6 +24,7 @@ pytestmark = pytest.mark.gpu
     ("elasticity", dict(n=10), api.ITER_BICGSTAB, 0),
     ("elasticity", dict(n=12), api.ITER_PIPECG, 0),
     ("laplacian", dict(n=20), api.ITER_PIPECG, 9),
+    ("elasticity", dict(n=12), api.ITER_GROPCG, 0),
 ])
 def test_sharded_path_one_rank_bit_identical(gpu, problem, kw, method, rr):
     """rr > 0: true residual every rr iterations (instead of 200), so the
@@ -72,6 +73,7 @@ def test_sharded_path_rejects_unsupported(gpu):
     ("elasticity", dict(n=7), api.ITER_CG),
     ("convection_diffusion", dict(n=14, peclet=5.0), api.ITER_BICGSTAB),
     ("laplacian", dict(n=14), api.ITER_PIPECG),
+    ("elasticity", dict(n=7), api.ITER_GROPCG),
 ])
 def test_sharded_boundary_rows_through_self_halo(gpu, problem, kw, method):
     """A one-rank system whose rows read some columns through ghost entries:

@@ -145,7 +145,7 @@ def test_unsupported_method_reports_status(product):
     elem = np.array([[0, 1]], dtype=np.int32)
     m.get_nonzero_pattern_by_simple_mesh(2, 2, 1, elem)
     m.quiet()
-    m.set_method(2)  # GropCG: not provided
+    m.set_method(4)  # PipeCR: not provided
     x = np.zeros(2)
     m.solve(np.ones(2), x)
     assert m.get_error_tag() == 5 and np.all(x == 0.0)

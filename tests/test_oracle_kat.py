@@ -36,9 +36,11 @@ def chain(lib, n_dof, rng, diag_shift=2.0):
 
 @pytest.mark.parametrize("n_dof", [1, 2, 3])
 @pytest.mark.parametrize("prec", [api.PREC_NONE, api.PREC_DIAG])
-@pytest.mark.parametrize("method,tol", [(api.ITER_CG, 1e-10), (api.ITER_BICGSTAB, 1e-12), (api.ITER_PIPECG, 1e-10)])
+@pytest.mark.parametrize("method,tol", [(api.ITER_CG, 1e-10), (api.ITER_BICGSTAB, 1e-12), (api.ITER_PIPECG, 1e-10),
+                                        (api.ITER_GROPCG, 1e-10)])
 def test_chain_solve_x_equals_one(oracle, n_dof, prec, method, tol):
-    # src_test/iterative/CG_test.f90:74-89, BiCGSTAB_test.f90 (tol 1e-12), PipeCG_test.f90:74-89
+    # src_test/iterative/CG_test.f90:74-89, BiCGSTAB_test.f90 (tol 1e-12), PipeCG_test.f90:74-89,
+    # GropCG_test.f90
     m = chain(oracle, n_dof, np.random.default_rng(10 * n_dof + prec))
     m.quiet()
     b = m.matvec(np.ones(10 * n_dof))
