@@ -86,6 +86,9 @@ struct SellMatrix {
   double bytes64 = 0, bytes32 = 0;   // HBM bytes of one SpMV in each layout
   // unroll depth (slots in flight per thread) picked by the autotuner
   int u64 = 2, u32 = 2;
+  // shape (N and ndof, NZ, padded slots) the depths were timed on: a rebuild
+  // of the same shape keeps them (the depth only affects speed)
+  long long tuned64[3] = {-1, -1, -1}, tuned32[3] = {-1, -1, -1};
   double* d_alu64 = nullptr;      // DIAG factors, entry-major: alu[e*N + row]
   float* d_alu32 = nullptr;
   // upload staging (kept between solves)
