@@ -11,7 +11,7 @@
 // on its rows.
 //
 // The host captures `batch` iterations into a CUDA graph and launches it
-// repeatedly, reading the state word once per launch with two launches in
+// repeatedly, reading the state word once per launch with three launches in
 // flight; kernels return immediately once `done` is set. The true residual
 // every iter_RR iterations of FP64 CG/BiCGSTAB falls on the last iteration of
 // a batch (the batch divides iter_RR) and uses a second graph that contains
