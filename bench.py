@@ -360,27 +360,46 @@ def workload_c4_sharded(lib, args, rank, world):
     """C4's independent systems over the ranks: replicas with no data-path
     collective (monolis_b200.partition.split_systems, greedy by stored
     blocks); every rank solves its share in one batch, FP32-refined to 1e-8;
-    the job time is the max over ranks."""
+    the job time is the max over ranks. Every rank reaches the same barrier
+    and reduction whatever happens locally (a rank without systems, or one
+    whose solve fails, reports 0 s or inf)."""
     from monolis_b200 import partition
     sides = problems.batch_sides(args.c4_count)
     share = partition.split_systems([7 * int(s) ** 3 for s in sides], world)[rank]
-    systems = [problems.fv_diffusion_csr(int(sides[i]), 4000 + i) for i in share]
-    bs = [problems.uniform(5000 + i, int(sides[i]) ** 3) for i in share]
-    batch = api.Batch(lib)
-    for ix, it, v, _ in systems:
-        batch.add_csr(len(ix) - 1, 1, ix, it, v)
-    batch.prepare(precond=api.PREC_DIAG, autotune=True)
-    batch.solve(bs, tol=1e-8, max_iter=20000, refine=True)  # warm-up; uploads b
+    t, err, converged, unknowns, batch = 0.0, None, True, 0, None
+    try:
+        if share:
+            systems = [problems.fv_diffusion_csr(int(sides[i]), 4000 + i) for i in share]
+            bs = [problems.uniform(5000 + i, int(sides[i]) ** 3) for i in share]
+            unknowns = int(sum(len(b) for b in bs))
+            batch = api.Batch(lib)
+            for ix, it, v, _ in systems:
+                batch.add_csr(len(ix) - 1, 1, ix, it, v)
+            batch.prepare(precond=api.PREC_DIAG, autotune=True)
+            batch.solve(bs, tol=1e-8, max_iter=20000, refine=True)  # warm-up; uploads b
+    except Exception as e:  # reported below, after the collectives every rank takes
+        err = repr(e)
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
-    _, _, st = batch.device_solve(tol=1e-8, max_iter=20000, refine=True)
-    t = batch.last_seconds()
-    batch.destroy()
-    return {"workload": f"{len(sides)} C4 systems over {world} ranks (greedy by stored blocks), FP32-refined 1e-8",
-            "systems_this_rank": len(share), "unknowns_this_rank": int(sum(len(b) for b in bs)),
-            "all_converged_this_rank": bool(np.all(st == 0)),
-            "s": max_over_ranks(t, world), "scaling": f"strong (the {len(sides)} systems are split)"}
+    try:
+        if batch is not None and err is None:
+            _, _, st = batch.device_solve(tol=1e-8, max_iter=20000, refine=True)
+            t = batch.last_seconds()
+            converged = bool(np.all(st == 0))
+    except Exception as e:
+        err = repr(e)
+    finally:
+        if batch is not None:
+            batch.destroy()
+    t_max = max_over_ranks(t if err is None else float("inf"), world)
+    out = {"workload": f"{len(sides)} C4 systems over {world} ranks (greedy by stored blocks), FP32-refined 1e-8",
+           "systems_this_rank": len(share), "unknowns_this_rank": unknowns,
+           "all_converged_this_rank": converged and err is None,
+           "s": t_max, "scaling": f"strong (the {len(sides)} systems are split)"}
+    if err is not None:
+        out["failed_this_rank"] = err
+    return out
 
 
 def multi_rhs_run(lib, sysm, rhs):
