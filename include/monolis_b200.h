@@ -33,7 +33,8 @@ static const int MONOLIS_B200_PRM_I_N_REFINE       = 33; /* out: FP64 residual r
 static const int MONOLIS_B200_PRM_I_BATCH          = 34; /* iterations per graph launch (0: 16) */
 static const int MONOLIS_B200_PRM_I_CHECK          = 35; /* 1: validate CSR index/item before upload */
 static const int MONOLIS_B200_PRM_I_LAUNCHES       = 36; /* out: kernels launched by the last solve */
-static const int MONOLIS_B200_PRM_I_ITER_RR        = 37; /* true-residual interval of CG/BiCGSTAB (0: 200, as the reference) */
+static const int MONOLIS_B200_PRM_I_ITER_RR        = 37; /* true-residual interval of CG/BiCGSTAB/PipeCG (0: the
+                                                            reference's 200, PipeCG 50; GropCG has none) */
 static const int MONOLIS_B200_PRM_I_UNROLL_FP64    = 38; /* out: SpMV unroll depth picked by the autotuner (FP64) */
 static const int MONOLIS_B200_PRM_I_UNROLL_FP32    = 39; /* out: same for the FP32 layout */
 static const int MONOLIS_B200_PRM_I_KERNEL_TIMERS  = 40; /* 1: time every kernel with CUDA events (no graph; slower loop);
