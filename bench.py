@@ -6,15 +6,21 @@ seeded perturbation), block CSR with ndof = 3 (2,097,152 block rows,
 55,742,968 3x3 blocks), CG + DIAG (3x3 block Jacobi), relative residual
 sqrt(<r,r>/<r0,r0>) < 1e-8. Inputs are synthetic (monolis_b200.problems).
 
-Our arm: the FP32-inner / FP64-refined CG (headline `value`, device-resident
-b and x), the plain FP64 CG beside it, standalone SpMV roofline figures, and
-`e2e` = the same solve through monolis_solve_R with host b/x (pinned), which
-includes uploading the matrix (the library re-uploads by default).
-`--impl reference`: the CPU oracle (restatement of the reference's CG) on the
-host cores, timed on a bounded sample of iterations and extrapolated to the
-oracle's iteration count for this system.
-Multi-GPU: independent replicas (one system per rank, weak scaling), time =
-max over ranks.
+Our arm (one GPU): headline `value` = the plain FP64 CG (the reference's
+arithmetic) with b and x resident in HBM, mean over the timed solves; `e2e` =
+the same FP64 solve through monolis_solve_R with pinned host b/x, which
+includes uploading the matrix (the library re-uploads by default), mean over
+the calls. Beside them: the FP32-inner / FP64-refined CG (`mixed`,
+`speedup_mixed_vs_fp64`), in-solve kernel times and the roofline of the
+dominant kernel, standalone SpMV figures, a bounded CPU-baseline sample and
+the secondary workloads (C3 BiCGSTAB, C4 batched / many right-hand sides, C5
+adjoint).
+`--impl reference`: the CPU oracle (restatement of the reference's FP64 CG)
+on every host core: one complete solve to 1e-8, measured whole and cut into
+`steps` consecutive iteration ranges by its per-iteration clock.
+Several GPUs: the system row-partitioned over the ranks (NCCL halo updates
+and all-reduced dot products, strong scaling, max over ranks); --replicas
+runs independent copies instead.
 """
 from __future__ import annotations
 
@@ -50,10 +56,13 @@ def workload_name(n, nz):
     return (f"3D linear elasticity {n}^3 nodes, hex8 Q1, E=1 nu=0.3, ndof=3, {nz} 3x3 blocks, "
             f"CG + 3x3 block-Jacobi, rel.res 1e-8")
 TOL = 1e-8
-# DRAM bytes (read + write) per launch of cg_spmv2_kernel divided by its
-# layout bytes, from the ncu --set full capture at 64^3 nodes
-# (271.92 MB / 268.45 MB); traffic scales with the blocks processed.
-NCU_SPMV2_TRAFFIC_RATIO = 1.0129
+# DRAM bytes (read + write) per launch of the FP64 cg_spmv_kernel divided by
+# its layout bytes, from the ncu --set full capture at 64^3 nodes
+# (527.12 MB / 522.13 MB); traffic scales with the blocks processed.
+NCU_SPMV64_TRAFFIC_RATIO = 1.0096
+NCU_SPMV64_TRAFFIC_SOURCE = ("ncu --set full capture of cg_spmv_kernel<3,3,double> at 64^3 nodes (dram read+write "
+                             "527.12 MB / layout bytes 522.13 MB = 1.0096), scaled by the layout bytes of a 128^3 "
+                             "launch")
 
 
 def log(*a):
@@ -554,10 +563,28 @@ def workload_c5(lib, args):
             "fd_directions": len(fd), "fd_max_rel_err_fp64": max(fd) if fd else None}
 
 
+def shared_config(n, nz, unknowns):
+    """The workload, identical in both arms' lines."""
+    mat_gb = nz * 9 * 8 / 1e9
+    l2 = (f"inputs larger than L2 (FP64 matrix {mat_gb:.1f} GB)" if mat_gb > 0.126
+          else f"matrix {mat_gb * 1e3:.0f} MB fits in L2")
+    return {"workload": workload_name(n, nz), "unknowns": int(unknowns), "nz_blocks": int(nz),
+            "arithmetic": "f64 (CG recurrences, SpMV, DIAG)", "l2": l2}
+
+
 def run_reference(args, rank):
-    """CPU oracle on the host cores: bounded sample, extrapolated."""
+    """The reference arm: the CPU oracle (the restatement of the reference's
+    FP64 CG, DIAG and SpMV) on every host core. One step is a contiguous
+    range of iterations of ONE complete solve to 1e-8: the solve is timed
+    whole, and the oracle's wall-clock log (end of every iteration) cuts it
+    into `steps` consecutive ranges, so `value` is a measured solve time and
+    steps x ms_per_step is the measured timed region. The warm-up is one
+    solve capped at `warmup` steps' worth of iterations. A single-threaded
+    sample (the reference's default build has no OpenMP) is reported beside
+    it, extrapolated by the iteration count, together with the fixture's
+    measured complete serial solve."""
     if rank != 0:
-        return
+        return  # other ranks of a multi-rank launch exit without work
     orc = api.load_library(ORACLE_SO, oracle=True)
     threads = os.cpu_count() or 1
     orc.oracle_set_threads(threads)
@@ -565,46 +592,129 @@ def run_reference(args, rank):
     t0 = time.perf_counter()
     b = problems.elasticity(m, n=args.n)
     t_asm = time.perf_counter() - t0
+    nz = int(m.csr_index()[-1])
     m.quiet()
     m.set_error_abort(False)
     m.set_method(api.ITER_CG)
     m.set_precond(api.PREC_DIAG)
     m.set_tolerance(TOL)
-    it_full = oracle_iterations(args.n)
-    if it_full is None and len(b) <= 200_000:
-        # no fixture for this size: a small system is solved to the end once
-        m.set_maxiter(20000)
-        x = np.zeros_like(b)
-        m.solve(b, x)
-        it_full = m.get_converge_iter()
-    sample_iters = args.cpu_sample_iters
-    m.set_maxiter(sample_iters)
-    per_step = []
-    for k in range(args.warmup + args.steps):
-        x = np.zeros_like(b)
-        t1 = time.perf_counter()
-        m.solve(b, x)
-        dt = time.perf_counter() - t1
-        if k >= args.warmup:
-            per_step.append(dt)
-    t_sample = float(np.median(per_step))
-    t_iter = t_sample / sample_iters
-    iters = it_full if it_full else None
-    value = t_iter * iters if iters else None
+    fx = fixture()
+    key = f"elasticity_n{args.n}_cg_diag_tol1e-08"
+    it_hint = fx.get(key) or 200
+    K = max(1, args.steps)
+    seg = max(1, -(-it_hint // K))
+    # warm-up: `warmup` steps of the timed steps' size
+    m.set_maxiter(max(1, args.warmup * seg))
+    x = np.zeros_like(b)
+    m.solve(b, x)
+    # timed: one complete solve with the iteration clock
+    max_iter = 20000
+    clock = np.zeros(max_iter + 2)
+    orc.oracle_set_iter_clock(api._dptr(clock), len(clock))
+    m.set_maxiter(max_iter)
+    x = np.zeros_like(b)
+    t1 = time.perf_counter()
+    m.solve(b, x)
+    t_solve = time.perf_counter() - t1
+    orc.oracle_set_iter_clock(None, 0)
+    it = m.get_converge_iter()
+    status = m.get_error_tag()
+    bounds = [round(k * it / K) for k in range(K + 1)]
+    step_s = [float(clock[bounds[k + 1]] - clock[bounds[k]]) for k in range(K)]
+    # single thread: a bounded sample of the same solve
+    orc.oracle_set_threads(1)
+    m.set_maxiter(args.cpu_sample_iters)
+    x1 = np.zeros_like(b)
+    t1 = time.perf_counter()
+    m.solve(b, x1)
+    t_1 = time.perf_counter() - t1
+    value = t_solve
     line = {
         "impl": "reference", "metric": metric_name(args.n), "value": value,
-        "unit": "s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": value * 1e3 if value else None, "higher_is_better": False, "scaling": "weak",
+        "unit": "s", "n_gpus": args.gpus, "steps": K, "warmup": args.warmup,
+        "ms_per_step": value / K * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name(args.n, int(m.csr_index()[-1])), "unknowns": int(len(b)),
-                   "nz_blocks": int(m.csr_index()[-1]), "parallelism": f"cpu, {threads} threads (oracle, FP64)"},
+        "config": shared_config(args.n, nz, len(b)),
+        "parallelism": f"cpu, {threads} threads (oracle, FP64)",
         "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": f"{sample_iters} CG iterations per step (median of {args.steps}), "
-                                   f"extrapolated x {iters} iterations (oracle count for this system)"},
+                         "sample": f"one complete FP64 CG + DIAG solve to rel.res 1e-8 ({it} iterations, "
+                                   f"status {status}) on {threads} threads, measured whole; steps are "
+                                   f"{K} consecutive iteration ranges of it"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "assembly_s": t_asm, "s_per_iteration": t_iter, "oracle_iterations": iters,
+        "iterations": it, "step_s": step_s, "assembly_s": t_asm,
+        "single_thread": {
+            "value_extrapolated": t_1 / args.cpu_sample_iters * it, "unit": "s", "cores": 1,
+            "sample": f"{args.cpu_sample_iters} iterations on 1 thread ({t_1:.2f} s), x {it} iterations",
+            "measured_full_solve_other_host": fx.get(key + ":seconds"),
+            "measured_full_solve_other_host_note": "complete serial oracle solve recorded by oracle/iterations.py "
+                                                   "on an 8-core Xeon @ 2.7 GHz (tests/golden)"},
     }
     print(json.dumps(line), flush=True)
+
+
+def timed_device_solves(m, stream, d_b, d_x, precision, warmup, steps, clock_index=None):
+    """warmup + steps device-resident solves (CUDA events on the library
+    stream); returns per-step seconds, iterations, launches, clocks."""
+    import torch
+    m.set_precision(precision)
+
+    def one():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = m.device_solve(d_b.data_ptr(), d_x.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        if rc != 0:
+            raise RuntimeError(f"solve failed: {api.STATUS_NAMES.get(rc, rc)}")
+        return e0.elapsed_time(e1) * 1e-3
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    times, iters, launches = [], [], 0
+    sampler = ClockSampler(clock_index) if clock_index is not None else None
+    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx-include "timed/" selects these launches
+    if sampler:
+        sampler.__enter__()
+    try:
+        for _ in range(steps):
+            times.append(one())
+            iters.append(m.get_converge_iter())
+            launches += int(m.Iarray[api.B200_PRM_I_LAUNCHES])
+    finally:
+        if sampler:
+            sampler.__exit__(None, None, None)
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    return times, iters, launches, (sampler.summary() if sampler else None)
+
+
+def e2e_calls(m, b, n_unk, precision, calls):
+    """monolis_solve_R with pinned host b and x, matrix uploaded by every
+    call (the library's default, like the reference's GPU build); one
+    untimed call first. Returns the per-call wall seconds."""
+    import torch
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.zeros(n_unk, dtype=torch.float64).pin_memory()
+    m.set_matrix_cache(False)
+    m.set_precision(precision)
+    out = []
+    for k in range(1 + calls):
+        hx.zero_()
+        t1 = time.perf_counter()
+        m.solve(hb.numpy(), hx.numpy())
+        dt = time.perf_counter() - t1
+        if m.get_error_tag() != 0:
+            raise RuntimeError(f"monolis_solve_R failed: status {m.get_error_tag()}")
+        if k >= 1:
+            out.append(dt)
+    return out
+
+
+def stats(v):
+    return {"mean_s": float(np.mean(v)), "median_s": float(np.median(v)), "max_s": float(np.max(v)),
+            "min_s": float(np.min(v)), "n": len(v)}
 
 
 def main():
@@ -615,9 +725,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=128)
     ap.add_argument("--cpu-sample-iters", type=int, default=10)
+    ap.add_argument("--cpu-baseline-iters", type=int, default=200,
+                    help="iterations of the CPU-baseline sample in our arm (about 10-30 s on the host)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workloads", default="c3,c4,c5",
                     help="secondary workloads to run after the headline (any of c3,c4,c5, or none)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: N independent copies of the headline system (weak scaling) instead of "
+                         "the row-partitioned solve of one system")
+    ap.add_argument("--sharded", action="store_true",
+                    help="force the row-partitioned multi-rank code path (NCCL halo + all-reduce), also at N = 1")
     ap.add_argument("--c4-count", type=int, default=512)
     ap.add_argument("--c4-sharded", action="store_true",
                     help="the C4 systems split over the N ranks (greedy by stored blocks), each rank "
@@ -636,7 +753,144 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank)
         return
+    if (world > 1 and not args.replicas) or args.sharded:
+        main_sharded(args, world, rank, local)
+    else:
+        main_ours(args, world, rank, local)
 
+
+def main_sharded(args, world, rank, local):
+    """The headline system row-partitioned over the ranks, the reference's
+    multi-rank model (src/linalg/matvec.f90:144: halo update before each
+    product; src/linalg/inner_product.f90:185: every dot product summed over
+    the ranks; src/solver/solver.f90:44: N = n_internal_vertex): contiguous
+    row ranges of about equal stored blocks (z-slabs of the structured mesh),
+    an NCCL communicator on the MONOLIS_COM of every rank, FP64 CG + DIAG
+    device-resident (monolis_b200_device_solve_com_R). Strong scaling: one
+    system, time = max over ranks. Every rank takes the same collective steps
+    in the same order, whatever happens locally."""
+    import datetime
+
+    # NCCL's own log of every communicator (ranks, devices, transports) on
+    # stderr, before the process group or the library creates one
+    os.environ.setdefault("NCCL_DEBUG", "INFO")
+    os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
+    import torch
+    import torch.distributed as dist
+
+    from monolis_b200 import partition
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    lib = api.load_product()
+    g = api.Monolis(lib)
+    t0 = time.perf_counter()
+    b = problems.elasticity(g, n=args.n)
+    nd, n_glob, nz_glob = g.NDOF, g.N, g.NZ
+    t1 = time.perf_counter()
+    p = partition.partition_rank(g.csr_index(), g.csr_item() - 1, g.values(), nd, world, rank)
+    t_part = time.perf_counter() - t1
+    rows = (p["glob"][:, None] * nd + np.arange(nd)[None, :]).reshape(-1)
+    b_loc = np.ascontiguousarray(b[rows])
+    g.finalize()
+    del g
+    m = api.Monolis(lib)
+    m.set_matrix_BCSR(p["N"], p["NP"], nd, len(p["item"]), p["val"], p["index"], p["item"])
+    m.quiet()
+    m.set_error_abort(False)
+    m.set_method(api.ITER_CG)
+    m.set_precond(api.PREC_DIAG)
+    m.set_tolerance(TOL)
+    m.set_maxiter(20000)
+    m.set_matrix_cache(True)
+    m.set_precision(0)
+    m.set_halo(p, rank, world)
+    # one NCCL unique id from rank 0 (through the process group's store)
+    uid = [api.nccl_unique_id(lib) if rank == 0 else None]
+    if world > 1:
+        dist.broadcast_object_list(uid, src=0)
+    m.com_init_nccl(uid[0], rank, world)
+    t_setup = time.perf_counter() - t0
+    log(f"[rank {rank}] rows {p['lo']}..{p['hi']} of {n_glob}, ghosts {p['NP'] - p['N']}, "
+        f"neighbours {list(p['recv_pe'])}, setup {t_setup:.1f}s (partition {t_part:.1f}s)")
+    stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+    d_b = torch.from_numpy(b_loc).cuda()
+    d_x = torch.zeros_like(d_b)
+    m.device_prepare()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def one():
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rc = m.device_solve_com(d_b.data_ptr(), d_x.data_ptr())
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) * 1e-3, rc
+
+    failed = None
+    for _ in range(args.warmup):
+        _, rc = one()
+        failed = failed or (rc or None)
+    barrier()
+    times, iters = [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t, rc = one()
+            failed = failed or (rc or None)
+            times.append(t)
+            iters.append(m.get_converge_iter())
+    barrier()
+    t_mean = float(np.mean(times)) if failed is None else float("inf")
+    t_max = max_over_ranks(t_mean, world)
+    it = int(np.median(iters))
+    res = m.get_converge_residual()
+    launches = int(m.Iarray[api.B200_PRM_I_LAUNCHES]) * args.steps
+    # e2e: monolis_solve_R with this rank's host b and x (pinned), device matrix kept
+    hb = torch.from_numpy(b_loc).pin_memory()
+    hx = torch.zeros(len(b_loc), dtype=torch.float64).pin_memory()
+    e2e = []
+    for k in range(1 + args.steps):
+        hx.zero_()
+        barrier()
+        t1 = time.perf_counter()
+        m.solve(hb.numpy(), hx.numpy())
+        if k >= 1:
+            e2e.append(time.perf_counter() - t1)
+    e2e_max = max_over_ranks(float(np.mean(e2e)), world)
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        line = {
+            "metric": metric_name(args.n), "value": t_max, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max * 1e3, "higher_is_better": False, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": shared_config(args.n, nz_glob, n_glob * nd),
+            "parallelism": f"row partition over {world} ranks (z-slabs; NCCL halo updates + all-reduced dots)",
+            "statistic": f"mean of {len(times)} solves, max over ranks", "iterations": it, "rel_residual": res,
+            "failed_status": failed,
+            "rank0": {"rows": int(p["N"]), "ghost_rows": int(p["NP"] - p["N"]),
+                      "neighbours": [int(v) for v in p["recv_pe"]], "step_s": times},
+            "e2e": {"value": e2e_max, "unit": "s",
+                    "h2d_bytes_per_step": int(len(b_loc) * 8), "d2h_bytes_per_step": int(len(b_loc) * 8),
+                    "path": "monolis_solve_R with the MONOLIS_COM (NCCL), pinned host b/x of rank 0's rows, "
+                            "device matrix kept (cache); bytes per step are rank 0's",
+                    "statistic": f"mean of {len(e2e)} calls, max over ranks", **stats(e2e)},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "roofline": None, "roofline_note": "see the one-GPU line (the same kernels on 1/N of the rows)",
+            "cpu_baseline": None, "peak_gbs": peak, "peak_kind": peak_kind,
+        }
+        print(json.dumps(line), flush=True)
+    m.finalize()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main_ours(args, world, rank, local):
     import torch
     import torch.distributed as dist
     torch.cuda.set_device(local)
@@ -664,72 +918,44 @@ def main():
     d_x = torch.zeros(n_unk, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
 
-    def timed_solve(precision):
-        m.set_precision(precision)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        rc = m.device_solve(d_b.data_ptr(), d_x.data_ptr())
-        e1.record(stream)
-        e1.synchronize()
-        if rc not in (0,):
-            raise RuntimeError(f"solve failed: {api.STATUS_NAMES.get(rc, rc)}")
-        return e0.elapsed_time(e1) * 1e-3, m.get_converge_iter(), m.get_converge_residual()
-
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # FP64 plain solver (reference semantics on the GPU); the device matrix is
-    # kept between the device-resident solves
+    # headline: the plain FP64 CG (the reference's arithmetic), device-resident
+    # b and x; the device matrix is kept between these solves
     m.set_matrix_cache(True)
     m.set_precision(0)
     m.device_prepare()
-    t64, it64, res64 = timed_solve(0)
-    t64, it64, res64 = timed_solve(0)
+    barrier()
+    t64s, it64s, launches, clocks = timed_device_solves(m, stream, d_b, d_x, 0, args.warmup, args.steps, local)
+    barrier()
+    t64 = float(np.mean(t64s))
+    it64 = int(np.median(it64s))
+    res64 = m.get_converge_residual()
     x64 = d_x.clone()
-    # mixed precision: warmup then timed steps
+    # the FP32-inner / FP64-refined CG on the same system
     m.set_precision(1)
     m.device_prepare()
-    for _ in range(args.warmup):
-        timed_solve(1)
-    times, iters = [], []
-    launches = 0
     barrier()
-    torch.cuda.nvtx.range_push("timed")  # ncu --nvtx-include "timed/" selects these launches
-    with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            t, it, res = timed_solve(1)
-            times.append(t)
-            iters.append(it)
-            launches += int(m.Iarray[api.B200_PRM_I_LAUNCHES])
-    torch.cuda.nvtx.range_pop()
+    t32s, it32s, _, clocks32 = timed_device_solves(m, stream, d_b, d_x, 1, max(2, args.warmup), args.steps, local)
     barrier()
-    clocks = clk.summary()
+    t_mixed = float(np.mean(t32s))
     nref = int(m.Iarray[api.B200_PRM_I_N_REFINE])  # FP64 refreshes of the last timed solve
-    # per-kernel durations inside a solve (kernel-timer mode, one extra solve
-    # of each precision, after the timed steps)
-    x_mixed = d_x.clone()
-    kt32, _ = kernel_times(m, stream, d_b, d_x)
-    m.set_precision(0)
-    kt64, _ = kernel_times(m, stream, d_b, d_x)
-    m.set_precision(1)
-    d_x.copy_(x_mixed)
-    t_mixed = float(np.mean(times))
     err_vs_fp64 = float(torch.linalg.norm(d_x - x64) / torch.linalg.norm(x64))
-    # true FP64 residual of the mixed solution (device FP64 SpMV)
     d_r = torch.empty_like(d_x)
     m.device_matvec(d_x.data_ptr(), d_r.data_ptr())
     stream.synchronize()
-    r0 = torch.linalg.norm(d_b).item()  # x0 = 0: r0 = b
-    true_res = torch.linalg.norm(d_b - d_r).item() / r0
+    true_res = torch.linalg.norm(d_b - d_r).item() / torch.linalg.norm(d_b).item()  # x0 = 0: r0 = b
+    # per-kernel durations inside a solve (kernel-timer mode, one extra solve of each precision)
+    kt32, _ = kernel_times(m, stream, d_b, d_x)
+    m.set_precision(0)
+    kt64, _ = kernel_times(m, stream, d_b, d_x)
 
     # SpMV roofline (standalone kernels, FP64 and FP32), CUDA events on the library stream
     nzb, padded, nslices = m.device_info()
     u64, u32 = int(m.Iarray[api.B200_PRM_I_UNROLL_FP64]), int(m.Iarray[api.B200_PRM_I_UNROLL_FP32])
-    # HBM bytes of one SpMV in the device layouts (16-bit column differences
-    # where a slice allows them), reported by the library after prepare
     layout_bytes = {"fp64": float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64]),
                     "fp32": float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP32])}
     layout = {"bytes_fp64": layout_bytes["fp64"], "bytes_fp32": layout_bytes["fp32"],
@@ -744,7 +970,7 @@ def main():
     torch.cuda.synchronize()
     spmv = {}
     reps = 20
-    for name, fp32, xs, ys, vb in (("fp64", False, xs64, ys64, 8), ("fp32", True, xs32, ys32, 4)):
+    for name, fp32, xs, ys in (("fp64", False, xs64, ys64), ("fp32", True, xs32, ys32)):
         for _ in range(3):
             m.device_matvec(xs.data_ptr(), ys.data_ptr(), fp32=fp32)
         e0 = torch.cuda.Event(enable_timing=True)
@@ -755,37 +981,22 @@ def main():
         e1.record(stream)
         e1.synchronize()
         dt = e0.elapsed_time(e1) * 1e-3 / reps
-        byts = layout_bytes[name]
-        spmv[name] = {"seconds": dt, "bytes": byts, "gbs": byts / dt / 1e9}
+        spmv[name] = {"seconds": dt, "bytes": layout_bytes[name], "gbs": layout_bytes[name] / dt / 1e9}
+    del xs64, ys64, xs32, ys32
     peak, peak_kind = measured_peak()
 
-    # device assembly of the same system (element matrices + clamped face),
-    # checked bit for bit against the host-assembled values
+    # device assembly of the same system, checked bit for bit against the host assembly
     asm = device_assembly_c2(lib, args.n, b)
 
     # e2e through monolis_solve_R with pinned host buffers (matrix upload included)
-    hb = torch.from_numpy(b).pin_memory()
-    hx = torch.zeros(n_unk, dtype=torch.float64).pin_memory()
-    m.set_matrix_cache(False)
-    m.set_precision(1)
-    e2e_times = []
-    for k in range(1 + args.steps):
-        hx.zero_()
-        t1 = time.perf_counter()
-        m.solve(hb.numpy(), hx.numpy())
-        dt = time.perf_counter() - t1
-        if k >= 1:
-            e2e_times.append(dt)
-    # median over the steps: the host side of a shared machine adds occasional
-    # spikes of a few hundred ms to single calls (mean and max reported too)
-    t_e2e = float(np.median(e2e_times))
+    e2e64 = e2e_calls(m, b, n_unk, 0, args.steps)
+    e2e32 = e2e_calls(m, b, n_unk, 1, min(args.steps, 5))
     h2d = nz * nd * nd * 8 + nz * 4 + (N + 1) * 4 + n_unk * 8  # values, items, offsets, b
     d2h = n_unk * 8
 
-    # max over ranks
-    t_mixed_max = max_over_ranks(t_mixed, world)
     t64_max = max_over_ranks(t64, world)
-    t_e2e_max = max_over_ranks(t_e2e, world)
+    t_mixed_max = max_over_ranks(t_mixed, world)
+    e2e64_max = max_over_ranks(float(np.mean(e2e64)), world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -801,15 +1012,15 @@ def main():
             mo.set_error_abort(False)
             mo.set_method(api.ITER_CG)
             mo.set_precond(api.PREC_DIAG)
-            mo.set_maxiter(args.cpu_sample_iters)
+            mo.set_maxiter(args.cpu_baseline_iters)
             xo = np.zeros_like(b)
             t1 = time.perf_counter()
             mo.solve(b, xo)
             t_s = time.perf_counter() - t1
-            t_it = t_s / args.cpu_sample_iters
+            t_it = t_s / args.cpu_baseline_iters
             cpu = {"value": t_it * it64, "unit": "s", "cores": threads, "kind": "port",
-                   "sample": f"{args.cpu_sample_iters} oracle CG iterations on the same system "
-                             f"({t_s:.2f} s), extrapolated x {it64} iterations"}
+                   "sample": f"{args.cpu_baseline_iters} oracle FP64 CG iterations on the same system "
+                             f"({t_s:.2f} s on {threads} threads), x {it64} iterations"}
             mo.finalize()
         except Exception as e:  # report, do not hide
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
@@ -837,18 +1048,18 @@ def main():
         spmv32_bytes = layout_bytes["fp32"]
         spmv64_bytes = layout_bytes["fp64"]
         in_solve = {
-            "mixed_us_per_iteration": {"p+fold": kt32[0] * 1e6, "q=A*p (fp32, +<p,q>)": kt32[1] * 1e6,
-                                       "update (+M^-1, dots)": kt32[2] * 1e6, "refresh (gated)": kt32[3] * 1e6},
             "fp64_us_per_iteration": {"p": kt64[0] * 1e6, "q=A*p (+<p,q>)": kt64[1] * 1e6,
                                       "update (+M^-1, dots)": kt64[2] * 1e6, "residual (gated)": kt64[3] * 1e6},
-            "spmv_fp32_in_solve_gbs": spmv32_bytes / kt32[1] / 1e9,
+            "mixed_us_per_iteration": {"p+fold": kt32[0] * 1e6, "q=A*p (fp32, +<p,q>)": kt32[1] * 1e6,
+                                       "update (+M^-1, dots)": kt32[2] * 1e6, "refresh (gated)": kt32[3] * 1e6},
             "spmv_fp64_in_solve_gbs": spmv64_bytes / kt64[1] / 1e9,
+            "spmv_fp32_in_solve_gbs": spmv32_bytes / kt32[1] / 1e9,
         }
         # solver roofline: the minimum fused CG schedule per iteration, {SpMV + <p,q>},
         # {x (y), r update, z = M^-1 r, <r,z>, <r,r>}, {p = z + beta p}: the SpMV bytes +
         # 12 vector passes + the block-Jacobi factors (9 per block row); the refined
         # solver adds its FP64 refreshes (FP64 SpMV + x, y, b, r, z and the factors)
-        it_mixed = int(np.median(iters))
+        it_mixed = int(np.median(it32s))
         bytes_it64 = spmv64_bytes + 12 * n_unk * 8 + 9 * N * 8
         bytes_it32 = spmv32_bytes + 12 * n_unk * 4 + 9 * N * 4
         bytes_refresh = spmv64_bytes + n_unk * (8 + 4 + 8 + 4 + 4) + 9 * N * 4
@@ -861,37 +1072,38 @@ def main():
                       "iterations": it_mixed, "achieved_gbs": total32 / t_mixed_max / 1e9,
                       "frac_of_measured": total32 / t_mixed_max / 1e9 / peak},
         }
+        achieved = in_solve["spmv_fp64_in_solve_gbs"]
         line = {
-            "metric": metric_name(args.n), "value": t_mixed_max, "unit": "s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_mixed_max * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic",
-            "config": {"workload": workload_name(args.n, nz),
-                       "unknowns": n_unk, "nz_blocks": nz, "padded_blocks": padded,
-                       "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (matrix 4.2 GB FP64 + 2.2 GB FP32)"},
-            "iterations": int(np.median(iters)), "fp64_refreshes": nref, "true_rel_residual": true_res,
-            "rel_error_vs_fp64_solution": err_vs_fp64,
-            "fp64": {"value": t64_max, "unit": "s", "iterations": it64, "rel_residual": res64},
-            "speedup_vs_fp64": t64_max / t_mixed_max,
+            "metric": metric_name(args.n), "value": t64_max, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t64_max * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": shared_config(args.n, nz, n_unk),
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "statistic": f"mean of {len(t64s)} solves", "step_s": t64s,
+            "iterations": it64, "rel_residual": res64,
+            "mixed": {"value": t_mixed_max, "unit": "s", "dtype": "f32 inner / f64 refinement",
+                      "iterations": it_mixed, "fp64_refreshes": nref, "true_rel_residual": true_res,
+                      "rel_error_vs_fp64_solution": err_vs_fp64, "statistic": f"mean of {len(t32s)} solves",
+                      "step_s": t32s, "clocks": clocks32,
+                      "e2e": {"value": float(np.mean(e2e32)), "unit": "s", **stats(e2e32)}},
+            "speedup_mixed_vs_fp64": t64_max / t_mixed_max,
             "spmv": {k: {"gbs": v["gbs"], "us": v["seconds"] * 1e6, "bytes": v["bytes"],
                          "frac_of_measured": v["gbs"] / peak, "frac_of_8tbs": v["gbs"] / 8000.0}
                      for k, v in spmv.items()},
-            "roofline": {"bound": "hbm", "achieved": in_solve["spmv_fp32_in_solve_gbs"], "peak": peak,
-                         "unit": "GB/s", "frac": in_solve["spmv_fp32_in_solve_gbs"] / peak,
-                         "traffic": NCU_SPMV2_TRAFFIC_RATIO * spmv32_bytes,
-                         "traffic_source": "ncu --set full capture of cg_spmv2_kernel at 64^3 nodes "
-                                           "(dram read+write / layout bytes = 1.013), scaled by the "
-                                           "layout bytes of a 128^3 launch",
-                         "kernel": "cg_spmv2_kernel (FP32 paired sliced-ELL SpMV q=A*p with fused <p,q>), "
-                                   "average launch inside a mixed solve, kernel-timer mode",
-                         "algorithmic_bytes_per_launch": spmv32_bytes, "peak_kind": peak_kind},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": (NCU_SPMV64_TRAFFIC_RATIO * spmv64_bytes
+                                     if NCU_SPMV64_TRAFFIC_RATIO else None),
+                         "traffic_source": NCU_SPMV64_TRAFFIC_SOURCE,
+                         "kernel": "cg_spmv_kernel (FP64 sliced-ELL SpMV q=A*p with the fused double-double "
+                                   "<p,q>), average launch inside an FP64 solve, kernel-timer mode",
+                         "algorithmic_bytes_per_launch": spmv64_bytes, "peak_kind": peak_kind},
             "in_solve_kernels": in_solve,
             "solver_roofline": solver_roofline,
             "spmv_layout": layout,
-            "e2e": {"value": t_e2e_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "path": "monolis_solve_R, pinned host b/x, matrix uploaded every call",
-                    "statistic": f"median of {len(e2e_times)} calls", "mean_s": float(np.mean(e2e_times)),
-                    "max_s": float(np.max(e2e_times))},
+            "e2e": {"value": e2e64_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "monolis_solve_R (FP64), pinned host b/x, matrix uploaded every call",
+                    "statistic": f"mean of {len(e2e64)} calls", **stats(e2e64)},
             "gpu_launches": launches,
             "autotuned_unroll": {"fp64": u64, "fp32": u32},
             "clocks": clocks,

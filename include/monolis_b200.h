@@ -44,6 +44,12 @@ static const int MONOLIS_B200_PRM_I_REFRESH_PERIOD = 41; /* mixed precision: FP6
 static const int MONOLIS_B200_PRM_I_WIDE_SLICES_FP64 = 42; /* out: 32-row slices that keep 32-bit column ids (the
                                                               others store 16-bit differences to a base per slot) */
 static const int MONOLIS_B200_PRM_I_WIDE_SLICES_FP32 = 43; /* out: same for the 64-row slices of the FP32 layout */
+static const int MONOLIS_B200_PRM_I_WAIT_LIMIT     = 44; /* many right-hand sides: polls after which a grid-barrier
+                                                            wait gives up and the solve returns MONOLIS_B200_TIMEOUT
+                                                            (0: 4,194,304, seconds) */
+static const int MONOLIS_B200_PRM_I_WAIT_DELAY_US  = 45; /* testing that bound: block 0 of the many-right-hand-side
+                                                            kernel reaches its first barrier this many microseconds
+                                                            late (0: off; at most 1,000,000) */
 
 static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
                                                             below delta * its largest value since the last one
@@ -100,6 +106,16 @@ int monolis_b200_device_prepare(MONOLIS* mat);
 /* Solve with b and x in device memory, using the prepared device matrix.
  * Synchronous; fills CUR_ITER, CUR_RESID, IERR and the timing slots. */
 int monolis_b200_device_solve_R(MONOLIS* mat, const double* d_b, double* d_x);
+
+/* The same with a MONOLIS_COM: when an NCCL communicator is attached to com
+ * (monolis_b200_com_init_nccl), the row-partitioned multi-rank FP64 solve of
+ * monolis_solve_R (halo updates through com's tables before each product,
+ * dot products all-reduced; src/linalg/matvec.f90:144,
+ * src/linalg/inner_product.f90:185) on device vectors of NP*NDOF entries,
+ * ghost rows last; otherwise monolis_b200_device_solve_R. Every rank calls it
+ * with the same parameters. Device-resident form of monolis_solve_R(mat, com,
+ * b, x) (wrapper/solver/monolis_solver_c.h:17). */
+int monolis_b200_device_solve_com_R(MONOLIS* mat, MONOLIS_COM* com, const double* d_b, double* d_x);
 
 /* y = A x with device vectors (asynchronous on the library stream). */
 int monolis_b200_device_matvec_R(MONOLIS* mat, const double* d_x, double* d_y);
@@ -222,6 +238,15 @@ int monolis_b200_device_set_Dirichlet_bc_R(MONOLIS* mat, double* d_b, int n_bc, 
                                            const int* n_dof_bc, const double* val);
 int monolis_b200_device_get_values(MONOLIS* mat, double* values);
 
+/* The FP64 DIAG factors of the prepared device matrix (the precond parameter
+ * DIAG when monolis_b200_device_prepare ran), written to alu (host, N*NDOF^2
+ * doubles) in the reference's layout: block of row i at alu[i*NDOF^2], its
+ * LU factors without pivoting, reciprocal pivots on the diagonal, a zero
+ * pivot replaced by 1 (src/prec/diag/diag_33.f90:16-99, diag_nn.f90:16-86).
+ * No counterpart in the reference's C API (its factors stay inside the
+ * solver); for checking the device setup against a host one. */
+int monolis_b200_device_get_diag(MONOLIS* mat, double* alu);
+
 /* ---- many right-hand sides on one matrix ----
  * No counterpart in the reference library (one right-hand side per solve).
  * Solves A X_k = B_k for k < n_rhs with CG and the struct's preconditioner
@@ -263,7 +288,10 @@ void monolis_b200_com_finalize_nccl(MONOLIS_COM* com);
  * device image, held by every GPU that loads the library until the process
  * exits, which caps n at 16,777,216 elements; larger n is rejected with
  * MONOLIS_B200_BAD_INPUT and an error message. The first call on each device
- * looks up that array's address (make it before any stream capture). All
+ * looks up that array's address (make it before any stream capture); the
+ * address is kept for the life of the process, so a cudaDeviceReset of a
+ * device on which this entry point has been called makes later calls on it
+ * invalid. All
  * calls share the one array: calls that overlap on the GPU (different
  * streams, or other host threads) race and must be serialised by the caller. */
 int monolis_b200_inner_product_noalloc_R(long long n, const double* d_x, const double* d_y, double* d_sum,

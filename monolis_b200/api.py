@@ -23,6 +23,7 @@ ITER_CG = 1
 ITER_GROPCG = 2
 ITER_PIPECG = 3
 ITER_BICGSTAB = 5
+ITER_BICGSTAB_N128 = 9
 PREC_NONE = 0
 PREC_DIAG = 1
 PRM_I_METHOD = 1
@@ -54,6 +55,8 @@ B200_PRM_I_KERNEL_TIMERS = 40
 B200_PRM_I_REFRESH_PERIOD = 41
 B200_PRM_I_WIDE_SLICES_FP64 = 42
 B200_PRM_I_WIDE_SLICES_FP32 = 43
+B200_PRM_I_WAIT_LIMIT = 44
+B200_PRM_I_WAIT_DELAY_US = 45
 B200_PRM_R_REFRESH_DELTA = 30
 B200_PRM_R_TIME_H2D = 31
 B200_PRM_R_TIME_D2H = 32
@@ -156,6 +159,7 @@ _PRODUCT = {
     "monolis_b200_stream": (C.c_void_p, []),
     "monolis_b200_device_prepare": (C.c_int, [_MP]),
     "monolis_b200_device_solve_R": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
+    "monolis_b200_device_solve_com_R": (C.c_int, [_MP, _CP, C.c_void_p, C.c_void_p]),
     "monolis_b200_device_matvec_R": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
     "monolis_b200_device_matvec_R32": (C.c_int, [_MP, C.c_void_p, C.c_void_p]),
     "monolis_b200_device_info": (C.c_int, [_MP, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
@@ -195,6 +199,7 @@ _PRODUCT = {
                                                      C.c_void_p]),
     "monolis_b200_device_set_Dirichlet_bc_R": (C.c_int, [_MP, C.c_void_p, C.c_int, _ip, _ip, _dp]),
     "monolis_b200_device_get_values": (C.c_int, [_MP, _dp]),
+    "monolis_b200_device_get_diag": (C.c_int, [_MP, _dp]),
     "monolis_b200_nccl_unique_id": (C.c_int, [C.c_void_p]),
     "monolis_b200_com_init_nccl": (C.c_int, [_CP, C.c_void_p, C.c_int, C.c_int]),
     "monolis_b200_com_finalize_nccl": (None, [_CP]),
@@ -205,12 +210,16 @@ _ORACLE_EXTRA = {
     "oracle_set_threads": (None, [C.c_int]),
     "oracle_get_threads": (C.c_int, []),
     "oracle_set_iter_rr": (None, [C.c_int]),
+    "oracle_set_iter_clock": (None, [_dp, C.c_int]),
     "oracle_pattern_by_simple_mesh_flat": (None, [_MP, C.c_int, C.c_int, C.c_int, C.c_int, _ip]),
     "oracle_add_elements": (None, [_MP, C.c_int, C.c_int, _ip, _dp, C.c_longlong, _dp]),
     "oracle_diag_setup": (None, [_MP, _dp]),
     "oracle_diag_apply": (None, [_MP, _dp, _dp, _dp]),
     "oracle_dot": (C.c_double, [C.c_longlong, _dp, _dp]),
     "oracle_sorted_dot": (C.c_double, [C.c_longlong, _dp, _dp]),
+    "oracle_dot_n128": (C.c_double, [C.c_longlong, _dp, _dp]),
+    "oracle_set_dot_mode": (None, [C.c_int]),
+    "oracle_get_dot_mode": (C.c_int, []),
     "oracle_check_converge": (C.c_int, [_MP, C.c_longlong, _dp, C.c_double, C.c_int]),
 }
 
@@ -557,6 +566,11 @@ class Monolis:
 
     def device_solve(self, d_b_ptr, d_x_ptr):
         return self.lib.monolis_b200_device_solve_R(self.p, C.c_void_p(d_b_ptr), C.c_void_p(d_x_ptr))
+
+    def device_solve_com(self, d_b_ptr, d_x_ptr):
+        """monolis_b200_device_solve_com_R with this struct's MONOLIS_COM."""
+        return self.lib.monolis_b200_device_solve_com_R(self.p, C.pointer(self.com), C.c_void_p(d_b_ptr),
+                                                        C.c_void_p(d_x_ptr))
 
     def device_matvec(self, d_x_ptr, d_y_ptr, fp32=False):
         fn = self.lib.monolis_b200_device_matvec_R32 if fp32 else self.lib.monolis_b200_device_matvec_R

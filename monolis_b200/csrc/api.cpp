@@ -463,7 +463,10 @@ int solve_resident(MONOLIS* m, DevState* s, mb::SellMatrix& A, const double* d_b
   int* I = m->prm.Iarray;
   double* R = m->prm.Rarray;
   mb::SolveParams p{};
-  p.method = I[MONOLIS_PRM_I_METHOD];
+  // BiCGSTAB_N128 (src/iterative/BiCGSTAB_N128.f90) is BiCGSTAB with
+  // double-double dot products; the device FP64 BiCGSTAB sums every dot
+  // product in double-double already
+  p.method = I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_BICGSTAB_N128 ? MONOLIS_ITER_BICGSTAB : I[MONOLIS_PRM_I_METHOD];
   p.precond = I[MONOLIS_PRM_I_PRECOND];
   p.max_iter = I[MONOLIS_PRM_I_MAX_ITER];
   p.tol = R[MONOLIS_PRM_R_TOL];
@@ -537,13 +540,15 @@ bool method_supported(const MONOLIS* m) {
   const int mth = m->prm.Iarray[MONOLIS_PRM_I_METHOD];
   const int pc = m->prm.Iarray[MONOLIS_PRM_I_PRECOND];
   if (mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG &&
-      mth != MONOLIS_ITER_GROPCG) {
+      mth != MONOLIS_ITER_GROPCG && mth != MONOLIS_ITER_BICGSTAB_N128) {
     fprintf(stderr,
-            "** monolis_b200: solver %s is not provided by this library (CG, GropCG, PipeCG, BiCGSTAB)\n",
+            "** monolis_b200: solver %s is not provided by this library (CG, GropCG, PipeCG, BiCGSTAB, "
+            "BiCGSTAB_N128)\n",
             str_iter(mth));
     return false;
   }
-  if ((mth == MONOLIS_ITER_PIPECG || mth == MONOLIS_ITER_GROPCG) && m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] != 0) {
+  if ((mth == MONOLIS_ITER_PIPECG || mth == MONOLIS_ITER_GROPCG || mth == MONOLIS_ITER_BICGSTAB_N128) &&
+      m->prm.Iarray[MONOLIS_B200_PRM_I_PRECISION] != 0) {
     fprintf(stderr, "** monolis_b200: %s runs in FP64 (MONOLIS_B200_PRECISION_FP64)\n", str_iter(mth));
     return false;
   }
@@ -898,18 +903,50 @@ void monolis_inner_product_R(MONOLIS* m, MONOLIS_COM* com, int n_dof, double* x,
 
 }  // extern "C"
 
+// The NCCL communicator attached to com (monolis_b200_com_init_nccl), or null.
+static void* nccl_comm_of(MONOLIS_COM* com) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  auto it = com ? nccl_comms().find(com) : nccl_comms().end();
+  return it != nccl_comms().end() ? it->second : nullptr;
+}
+
+// Methods and precisions of the multi-rank solve.
+static bool sharded_supported(const MONOLIS* m) {
+  const int* I = m->prm.Iarray;
+  const int mth = I[MONOLIS_PRM_I_METHOD];
+  if ((mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG &&
+       mth != MONOLIS_ITER_GROPCG) ||
+      I[MONOLIS_B200_PRM_I_PRECISION] != 0) {
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB)\n");
+    return false;
+  }
+  return true;
+}
+
+// Halo plan of the rank-local system from the MONOLIS_COM tables
+// (src/linalg/matvec.f90:144 updates the ghost entries through them);
+// caller holds g_ctx_mu and has prepared s->A.
+static int attach_shard(MONOLIS* m, DevState* s, MONOLIS_COM* com, void* ncomm) {
+  mb::ShardTables t;
+  t.rank = com->my_rank;
+  t.send_pe.assign(com->send_neib_pe, com->send_neib_pe + com->send_n_neib);
+  t.send_ptr.assign(com->send_index, com->send_index + com->send_n_neib + 1);
+  t.send_item.assign(com->send_item, com->send_item + (com->send_n_neib ? com->send_index[com->send_n_neib] : 0));
+  t.recv_pe.assign(com->recv_neib_pe, com->recv_neib_pe + com->recv_n_neib);
+  t.recv_ptr.assign(com->recv_index, com->recv_index + com->recv_n_neib + 1);
+  t.recv_item.assign(com->recv_item, com->recv_item + (com->recv_n_neib ? com->recv_index[com->recv_n_neib] : 0));
+  int rc = mb::shard_setup(s->shard, t, m->mat.NDOF, s->A, ctx().stream);
+  s->shard.comm = ncomm;
+  return rc;
+}
+
 // src/solver/solver.f90:29-49 + wrapper/solver/monolis_solver_c.c:8-60, for A
 // or (transpose) A^T.
 static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool transpose) {
   const double t_start = now_sec();
   int* I = m->prm.Iarray;
   // multi-rank: an NCCL communicator attached with monolis_b200_com_init_nccl
-  void* ncomm = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(g_ctx_mu);
-    auto it = com ? nccl_comms().find(com) : nccl_comms().end();
-    if (it != nccl_comms().end()) ncomm = it->second;
-  }
+  void* ncomm = nccl_comm_of(com);
   if (com && com->comm_size > 1 && !ncomm) {
     fprintf(stderr, "** monolis_b200: comm_size=%d needs an NCCL communicator (monolis_b200_com_init_nccl)\n",
             com->comm_size);
@@ -917,11 +954,7 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
     return MONOLIS_B200_BAD_INPUT;
   }
   const bool sharded = ncomm != nullptr;
-  if (sharded && (transpose ||
-                  (I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_CG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_BICGSTAB &&
-                   I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_PIPECG && I[MONOLIS_PRM_I_METHOD] != MONOLIS_ITER_GROPCG) ||
-                  I[MONOLIS_B200_PRM_I_PRECISION] != 0)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB)\n");
+  if (sharded && (transpose || !sharded_supported(m))) {
     I[MONOLIS_PRM_I_IERR] = MONOLIS_B200_BAD_INPUT;
     return MONOLIS_B200_BAD_INPUT;
   }
@@ -943,18 +976,7 @@ static int solve_host(MONOLIS* m, MONOLIS_COM* com, double* b, double* x, bool t
   // multi-rank: x and b hold the ghost rows too (NP)
   const size_t n = (size_t)(sharded ? m->mat.NP : m->mat.N) * m->mat.NDOF;
   if (!rc) rc = ensure_vec(s, n);
-  if (!rc && sharded) {
-    mb::ShardTables t;
-    t.rank = com->my_rank;
-    t.send_pe.assign(com->send_neib_pe, com->send_neib_pe + com->send_n_neib);
-    t.send_ptr.assign(com->send_index, com->send_index + com->send_n_neib + 1);
-    t.send_item.assign(com->send_item, com->send_item + (com->send_n_neib ? com->send_index[com->send_n_neib] : 0));
-    t.recv_pe.assign(com->recv_neib_pe, com->recv_neib_pe + com->recv_n_neib);
-    t.recv_ptr.assign(com->recv_index, com->recv_index + com->recv_n_neib + 1);
-    t.recv_item.assign(com->recv_item, com->recv_item + (com->recv_n_neib ? com->recv_index[com->recv_n_neib] : 0));
-    rc = mb::shard_setup(s->shard, t, m->mat.NDOF, s->A, ctx().stream);
-    s->shard.comm = ncomm;
-  }
+  if (!rc && sharded) rc = attach_shard(m, s, com, ncomm);
   if (rc) {
     I[MONOLIS_PRM_I_IERR] = rc;
     return rc;
@@ -1080,6 +1102,28 @@ int monolis_b200_device_solve_R(MONOLIS* m, const double* d_b, double* d_x) {
   return m->prm.Iarray[MONOLIS_PRM_I_IERR];
 }
 
+int monolis_b200_device_solve_com_R(MONOLIS* m, MONOLIS_COM* com, const double* d_b, double* d_x) {
+  const double t_start = now_sec();
+  void* ncomm = nccl_comm_of(com);
+  if (!ncomm) return monolis_b200_device_solve_R(m, d_b, d_x);
+  if (!method_supported(m) || !sharded_supported(m)) return MONOLIS_B200_BAD_INPUT;
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared) return MONOLIS_B200_BAD_INPUT;
+  const int* I = m->prm.Iarray;
+  if (I[MONOLIS_PRM_I_PRECOND] == MONOLIS_PREC_DIAG && !s->A.have_alu) {
+    int rc = mb::diag_setup(s->A, ctx().stream);
+    if (rc) return rc;
+  }
+  int rc = attach_shard(m, s, com, ncomm);
+  if (rc) return rc;
+  rc = solve_resident(m, s, s->A, d_b, d_x, t_start, 0.0, 0.0, &s->shard);
+  if (rc) return rc;
+  print_summary(m);
+  return m->prm.Iarray[MONOLIS_PRM_I_IERR];
+}
+
 int monolis_b200_device_solve_transpose_R(MONOLIS* m, const double* d_b, double* d_x) {
   const double t_start = now_sec();
   if (!method_supported(m)) return MONOLIS_B200_BAD_INPUT;
@@ -1115,7 +1159,10 @@ int monolis_b200_device_solve_multi_R(MONOLIS* m, int n_rhs, const double* d_B, 
   const double t0 = now_sec();
   rc = mb::multi_solve(s->A, *s->multi, s->build_id, n_rhs, d_B, d_X, mixed ? 1 : 0, pc == MONOLIS_PREC_DIAG ? 1 : 0,
                        m->prm.Rarray[MONOLIS_PRM_R_TOL], I[MONOLIS_PRM_I_MAX_ITER],
-                       m->prm.Rarray[MONOLIS_B200_PRM_R_REFRESH_DELTA], iter, resid, status, ctx().stream);
+                       m->prm.Rarray[MONOLIS_B200_PRM_R_REFRESH_DELTA],
+                       (unsigned long long)std::max(I[MONOLIS_B200_PRM_I_WAIT_LIMIT], 0),
+                       (unsigned int)std::min(std::max(I[MONOLIS_B200_PRM_I_WAIT_DELAY_US], 0), 1000000) * 1000u,
+                       iter, resid, status, ctx().stream);
   m->prm.Rarray[MONOLIS_B200_PRM_R_TIME_LOOP] = now_sec() - t0;
   I[MONOLIS_PRM_I_IERR] = rc;
   return rc;
@@ -1206,6 +1253,23 @@ int monolis_b200_device_get_values(MONOLIS* m, double* values) {
   const size_t nv = (size_t)s->A.nz * s->A.ndof * s->A.ndof;
   MB_API_CUDA(cudaMemcpyAsync(values, s->A.d_csrval, nv * sizeof(double), cudaMemcpyDeviceToHost, ctx().stream));
   MB_API_CUDA(cudaStreamSynchronize(ctx().stream));
+  return MONOLIS_B200_OK;
+}
+
+int monolis_b200_device_get_diag(MONOLIS* m, double* alu) {
+  std::lock_guard<std::mutex> lk(g_ctx_mu);
+  if (ctx_init()) return MONOLIS_B200_CUDA_ERROR;
+  DevState* s = state_of(m);
+  if (!s->prepared || !s->A.have_alu || !alu) return MONOLIS_B200_BAD_INPUT;
+  const int N = s->A.N, nd2 = s->A.ndof * s->A.ndof;
+  std::vector<double> dev((size_t)nd2 * N);
+  MB_API_CUDA(cudaMemcpyAsync(dev.data(), s->A.d_alu64, dev.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              ctx().stream));
+  MB_API_CUDA(cudaStreamSynchronize(ctx().stream));
+  // device storage is entry-major (alu[e*N + row]); the reference's is
+  // block by block (ALU(nd2*(row-1) + e))
+  for (int row = 0; row < N; row++)
+    for (int e = 0; e < nd2; e++) alu[(size_t)row * nd2 + e] = dev[(size_t)e * N + row];
   return MONOLIS_B200_OK;
 }
 

@@ -101,7 +101,7 @@ struct SellMatrix {
 };
 
 struct Scratch {
-  double* partials = nullptr;     // kMaxBlocks * 4 doubles
+  double* partials = nullptr;     // (65536 + 256) * 4 doubles: block and group partial sums
   unsigned int* ticket = nullptr;
   SolverState* st = nullptr;
   SolverState* h_st = nullptr;    // pinned host mirror
@@ -225,9 +225,12 @@ void multi_free(MultiState* ms);
 // n_rhs systems A X_k = B_k with B_k at d_B + k*N*ndof (device); precision 1:
 // FP32 loop with FP64 refresh, 0: FP64. build_id identifies the device
 // matrix contents (the FP32 CSR copy is rebuilt when it changes).
+// wait_limit: polls before a grid-barrier wait gives up (0: the default,
+// seconds); delay_ns: testing, block 0 arrives that much later at the first
+// barrier. A wait that gives up ends the solve with kTimeout.
 int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, const double* d_B, double* d_X,
-                int precision, int prec, double tol, int max_iter, double delta, int* iter, double* resid,
-                int* status, cudaStream_t s);
+                int precision, int prec, double tol, int max_iter, double delta, unsigned long long wait_limit,
+                unsigned int delay_ns, int* iter, double* resid, int* status, cudaStream_t s);
 
 int scratch_ensure(Scratch& sc, size_t hist_len);
 void scratch_free(Scratch& sc);

@@ -24,6 +24,7 @@
 // reliable updates r = b - A (x + y) in FP64; FP64: the same loop in double.
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "monolis_b200.h"
@@ -34,7 +35,8 @@ namespace {
 
 constexpr int kMultiK = 32;
 constexpr int kMultiThreads = 256;
-constexpr unsigned long long kSpinLimit = 1ull << 22;  // polls (an L2 round trip + 32 ns each): seconds
+// default bound of every barrier wait: polls of an L2 round trip + 32 ns each, seconds in all
+constexpr unsigned long long kSpinLimit = 1ull << 22;
 
 constexpr int kBarrierGroup = 32;  // blocks per first-level group of the barrier
 constexpr int kMaxGroups = 128;
@@ -66,6 +68,8 @@ struct MultiArgs {
   T *y, *r, *z, *p0, *p1, *q;
   double* partials;    // [gridDim.x][2][32]
   MultiCtl* ctl;
+  unsigned long long spin_limit;  // polls before a barrier wait gives up
+  unsigned int delay_ns;          // testing: block 0 arrives this much later at the first barrier
 };
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
@@ -86,7 +90,8 @@ __device__ __forceinline__ void st_release(unsigned int* p, unsigned int v) {
 // adds at most one group's worth of values, so the barrier's tail stays short.
 // Waits are bounded; returns false once any block has given up.
 template <class F>
-__device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*tot)[kMultiK], F&& last) {
+__device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*tot)[kMultiK],
+                          unsigned long long limit, F&& last) {
   __shared__ unsigned int s_grel, s_gen;
   __shared__ int s_role, s_ok;  // 0: wait for the group, 1: group finisher, 2: last block
   const unsigned int G = gridDim.x, g = blockIdx.x / kBarrierGroup;
@@ -140,7 +145,7 @@ __device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*t
       // group finisher: wait for the global release (at most ngroups pollers)
       unsigned long long n = 0;
       while (ld_acquire(&c->gen) == s_gen) {
-        if (++n > kSpinLimit) {
+        if (++n > limit) {
           atomicExch(&c->err, 1);
           break;
         }
@@ -153,7 +158,7 @@ __device__ bool grid_sync(MultiCtl* c, double* partials, bool reduce, double (*t
     // wait for this group's release (at most kBarrierGroup pollers per line)
     unsigned long long n = 0;
     while (ld_acquire(grel) == s_grel) {
-      if (++n > kSpinLimit) {
+      if (++n > limit) {
         atomicExch(&c->err, 1);
         break;
       }
@@ -382,15 +387,20 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
     reduce_write(v0, v1);
   };
 
+  // testing: block 0 late at the first barrier (bounded sleep), so that the
+  // other blocks' waits run out when the limit is shorter
+  if (a.delay_ns && blockIdx.x == 0 && threadIdx.x == 0) {
+    for (unsigned int t = 0; t < a.delay_ns; t += 1000) __nanosleep(1000);
+  }
   // the whole grid has zeroed its x and y before any residual reads them
-  if (!grid_sync(c, a.partials, false, s_tot, [] {})) return;
+  if (!grid_sync(c, a.partials, false, s_tot, a.spin_limit, [] {})) return;
   {
     bool all[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) all[j] = 4 * qd + j < K;
     refresh(all);
   }
-  if (!grid_sync(c, a.partials, true, s_tot, [&] {
+  if (!grid_sync(c, a.partials, true, s_tot, a.spin_limit, [&] {
         if (threadIdx.x < kMultiK) {
           const int kk = threadIdx.x;
           const double rr = s_tot[0][kk], rz = s_tot[1][kk];
@@ -504,7 +514,7 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
       }
     }
     reduce_write(pq, zero4);
-    if (!grid_sync(c, a.partials, true, s_tot, [&] {
+    if (!grid_sync(c, a.partials, true, s_tot, a.spin_limit, [&] {
           if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
             const double w = s_tot[0][kk];
@@ -574,7 +584,7 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
       }
       reduce_write(v0, v1);
     }
-    if (!grid_sync(c, a.partials, true, s_tot, [&] {
+    if (!grid_sync(c, a.partials, true, s_tot, a.spin_limit, [&] {
           int any_r = 0;
           if (threadIdx.x < K && !vc->done[threadIdx.x]) {
             const int kk = threadIdx.x;
@@ -614,7 +624,7 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
         mine[j] = k < K && __ldcg(&c->refresh[k]) != 0;
       }
       refresh(mine);
-      if (!grid_sync(c, a.partials, true, s_tot, [&] {
+      if (!grid_sync(c, a.partials, true, s_tot, a.spin_limit, [&] {
             if (threadIdx.x < K && vc->refresh[threadIdx.x]) {
               const int kk = threadIdx.x;
               const double rr = s_tot[0][kk], rz = s_tot[1][kk];
@@ -723,9 +733,14 @@ cudaError_t grow_m(P** p, size_t& cap, size_t need) {
   return e;
 }
 
+// The chunk's work as one CUDA graph: right-hand sides to the interleaved
+// layout, control block cleared, the persistent kernel (cooperative launch:
+// every block resident), solutions back to the caller's layout.
 template <int B, class T, int Q>
-int launch_multi(const MultiArgs<T>& args, cudaStream_t s) {
+int capture_multi(const MultiArgs<T>& args, const double* d_B, double* b_dst, double* d_X, long long ld, int Kc,
+                  cudaStream_t s, cudaGraph_t* graph) {
   auto kernel = multi_cg_kernel<B, T, Q>;
+  constexpr int Kp = 4 * Q;
   int per_sm = 0, dev = 0, sms = 0;
   MB_CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kMultiThreads, 0));
   MB_CUDA_OK(cudaGetDevice(&dev));
@@ -733,7 +748,6 @@ int launch_multi(const MultiArgs<T>& args, cudaStream_t s) {
   if (per_sm < 1) return kBadInput;
   // every block resident (cooperative launch), within the barrier's group table
   const int grid = std::min(per_sm * sms, kMaxGroups * kBarrierGroup);
-  MultiArgs<T> a = args;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -743,8 +757,23 @@ int launch_multi(const MultiArgs<T>& args, cudaStream_t s) {
   cfg.stream = s;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  MB_CUDA_OK(cudaMemsetAsync(a.ctl, 0, sizeof(MultiCtl), s));
-  MB_CUDA_OK(cudaLaunchKernelEx(&cfg, kernel, a));
+  MB_CUDA_OK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  to_interleaved<<<148 * 8, 256, 0, s>>>(d_B, b_dst, ld, Kc, Kp, ld);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemsetAsync(args.ctl, 0, sizeof(MultiCtl), s);
+  if (e == cudaSuccess) e = cudaLaunchKernelEx(&cfg, kernel, args);
+  if (e == cudaSuccess) {
+    from_interleaved<<<148 * 8, 256, 0, s>>>(args.x, d_X, ld, Kc, Kp, ld);
+    e = cudaGetLastError();
+  }
+  // the capture is always ended, so the stream stays usable after an error
+  const cudaError_t e2 = cudaStreamEndCapture(s, graph);
+  if (e != cudaSuccess) {
+    if (*graph) cudaGraphDestroy(*graph);
+    *graph = nullptr;
+    return report_cuda(e, "multi-RHS launch sequence (stream capture)", __FILE__, __LINE__);
+  }
+  if (e2 != cudaSuccess) return report_cuda(e2, "cudaStreamEndCapture (multi-RHS graph)", __FILE__, __LINE__);
   return kOk;
 }
 
@@ -759,11 +788,19 @@ struct MultiState {
   MultiCtl* ctl = nullptr;
   size_t cap_b = 0, cap_x = 0, cap_vec = 0, cap_part = 0;
   long long built_for = -1;
+  // instantiated graphs of recent chunk launches, keyed by every argument
+  // of the launch sequence (a repeated solve relaunches its graph)
+  struct Slot {
+    std::vector<unsigned char> key;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::vector<Slot> graphs;
 };
 
 MultiState* multi_new() { return new MultiState(); }
 void multi_free(MultiState* ms) {
   if (!ms) return;
+  for (auto& g : ms->graphs) cudaGraphExecDestroy(g.exec);
   cudaFree(ms->col);
   cudaFree(ms->val32);
   cudaFree(ms->b);
@@ -776,10 +813,19 @@ void multi_free(MultiState* ms) {
 
 // Solve A X_k = B_k for n_rhs right-hand sides stored one after another
 // (B + k*ld, ld = N*ndof), in chunks of up to 32.
+namespace {
+template <class P>
+void append_bytes(std::vector<unsigned char>& k, const P& v) {
+  const unsigned char* p = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), p, p + sizeof(P));
+}
+}  // namespace
+
 int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, const double* d_B, double* d_X,
-                int precision, int prec, double tol, int max_iter, double delta, int* iter, double* resid, int* status,
-                cudaStream_t s) {
+                int precision, int prec, double tol, int max_iter, double delta, unsigned long long wait_limit,
+                unsigned int delay_ns, int* iter, double* resid, int* status, cudaStream_t s) {
   if (n_rhs < 1 || max_iter < 1 || !(tol >= 0.0)) return kBadInput;
+  if (wait_limit == 0) wait_limit = kSpinLimit;
   if (prec && !m.have_alu) return kBadInput;
   if (precision == 1 && prec && !m.have_alu32) return kBadInput;
   const int N = m.N, nd = m.ndof, B2 = nd * nd;
@@ -813,34 +859,66 @@ int multi_solve(SellMatrix& m, MultiState& ms, long long build_id, int n_rhs, co
   for (int k0 = 0; k0 < n_rhs; k0 += kMultiK) {
     const int Kc = std::min(kMultiK, n_rhs - k0);
     const int Q = Kc <= 8 ? 2 : 8;  // lanes per row; right-hand sides padded to 4Q
-    const int Kp = 4 * Q;
-    to_interleaved<<<148 * 8, 256, 0, s>>>(d_B + (long long)k0 * ld, ms.b, ld, Kc, Kp, ld);
+    const double* Bk = d_B + (long long)k0 * ld;
+    double* Xk = d_X + (long long)k0 * ld;
     char* v = static_cast<char*>(ms.vec);
+    // the launch arguments, zero-filled first so that padding bytes compare equal in the key
+    std::vector<unsigned char> key;
+    cudaGraph_t graph = nullptr;
     int rc = dispatch_ndof(nd, [&](auto Bc) -> int {
       constexpr int Bn = decltype(Bc)::value;
+      append_bytes(key, Bn);
+      append_bytes(key, Q);
+      append_bytes(key, precision);
+      append_bytes(key, Bk);
+      append_bytes(key, Xk);
+      append_bytes(key, ld);
+      append_bytes(key, s);
       if (precision == 1) {
-        MultiArgs<float> a{};
+        MultiArgs<float> a;
+        memset(&a, 0, sizeof(a));
         a.N = N; a.K = Kc; a.prec = prec; a.refine = 1; a.max_iter = max_iter; a.tol = tol;
         a.delta = delta > 0 ? delta : 0.1;
         a.rowptr = m.d_rowptr; a.col = ms.col; a.val = ms.val32; a.val64 = m.d_csrval; a.alu = m.d_alu32;
         a.b = ms.b; a.x = ms.x;
         a.y = (float*)(v); a.r = (float*)(v + vec_bytes); a.z = (float*)(v + 2 * vec_bytes);
         a.p0 = (float*)(v + 3 * vec_bytes); a.p1 = (float*)(v + 4 * vec_bytes); a.q = (float*)(v + 5 * vec_bytes);
-        a.partials = ms.partials; a.ctl = ms.ctl;
-        return Q == 2 ? launch_multi<Bn, float, 2>(a, s) : launch_multi<Bn, float, 8>(a, s);
+        a.partials = ms.partials; a.ctl = ms.ctl; a.spin_limit = wait_limit; a.delay_ns = delay_ns;
+        append_bytes(key, a);
+        for (auto& g : ms.graphs)
+          if (g.key == key) return kOk;
+        return Q == 2 ? capture_multi<Bn, float, 2>(a, Bk, ms.b, Xk, ld, Kc, s, &graph)
+                      : capture_multi<Bn, float, 8>(a, Bk, ms.b, Xk, ld, Kc, s, &graph);
       }
-      MultiArgs<double> a{};
+      MultiArgs<double> a;
+      memset(&a, 0, sizeof(a));
       a.N = N; a.K = Kc; a.prec = prec; a.refine = 0; a.max_iter = max_iter; a.tol = tol; a.delta = 0.1;
       a.rowptr = m.d_rowptr; a.col = ms.col; a.val = m.d_csrval; a.val64 = m.d_csrval; a.alu = m.d_alu64;
       a.b = ms.b; a.x = ms.x;
       a.y = (double*)(v); a.r = (double*)(v + vec_bytes); a.z = (double*)(v + 2 * vec_bytes);
       a.p0 = (double*)(v + 3 * vec_bytes); a.p1 = (double*)(v + 4 * vec_bytes); a.q = (double*)(v + 5 * vec_bytes);
-      a.partials = ms.partials; a.ctl = ms.ctl;
-      return Q == 2 ? launch_multi<Bn, double, 2>(a, s) : launch_multi<Bn, double, 8>(a, s);
+      a.partials = ms.partials; a.ctl = ms.ctl; a.spin_limit = wait_limit; a.delay_ns = delay_ns;
+      append_bytes(key, a);
+      for (auto& g : ms.graphs)
+        if (g.key == key) return kOk;
+      return Q == 2 ? capture_multi<Bn, double, 2>(a, Bk, ms.b, Xk, ld, Kc, s, &graph)
+                    : capture_multi<Bn, double, 8>(a, Bk, ms.b, Xk, ld, Kc, s, &graph);
     });
     if (rc) return rc;
-    from_interleaved<<<148 * 8, 256, 0, s>>>(ms.x, d_X + (long long)k0 * ld, ld, Kc, Kp, ld);
-    MB_CUDA_OK(cudaGetLastError());
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : ms.graphs)
+      if (g.key == key) exec = g.exec;
+    if (!exec) {
+      const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return report_cuda(e, "cudaGraphInstantiate (multi-RHS graph)", __FILE__, __LINE__);
+      if (ms.graphs.size() >= 8) {
+        cudaGraphExecDestroy(ms.graphs.front().exec);
+        ms.graphs.erase(ms.graphs.begin());
+      }
+      ms.graphs.push_back({key, exec});
+    }
+    MB_CUDA_OK(cudaGraphLaunch(exec, s));
     MB_CUDA_OK(cudaMemcpyAsync(h.data(), ms.ctl, sizeof(MultiCtl), cudaMemcpyDeviceToHost, s));
     MB_CUDA_OK(cudaStreamSynchronize(s));
     if (h[0].err) {

@@ -266,9 +266,9 @@ int persistent_blocks(K kernel) {
 template <class T>
 __global__ void dot_kernel(long long n, const T* __restrict__ x, const T* __restrict__ y, double* partials,
                            unsigned int* ticket, double* out) {
-  double v[1] = {0.0};
+  DotAcc<1, T> v;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    v[0] += (double)x[i] * (double)y[i];
+    v.add(0, x[i], y[i]);
   grid_reduce<1>(v, partials, ticket, [&](double* tot) { *out = tot[0]; });
 }
 
@@ -573,7 +573,8 @@ int sell_autotune(SellMatrix& m, bool fp32, cudaStream_t s) {
 }
 
 int scratch_ensure(Scratch& sc, size_t hist_len) {
-  const size_t need = 65536 * 4;
+  // up to 65536 blocks of 4 doubles, or of 2 double-double sums
+  const size_t need = (65536 + 256) * 4;
   if (sc.partials_cap < need) {
     if (sc.partials) cudaFree(sc.partials);
     MB_CUDA_OK(cudaMalloc((void**)&sc.partials, need * sizeof(double)));
@@ -605,6 +606,7 @@ void scratch_free(Scratch& sc) {
 int dot64(long long n, const double* x, const double* y, double* out, Scratch& sc, cudaStream_t s) {
   int rc = scratch_ensure(sc, 1);
   if (rc) return rc;
+  MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * kTicketWords, s));
   dot_kernel<double><<<148 * 4, 256, 0, s>>>(n, x, y, sc.partials, sc.ticket, out);
   MB_CUDA_OK(cudaGetLastError());
   return kOk;

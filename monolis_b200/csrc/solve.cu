@@ -177,7 +177,8 @@ __device__ void fin_pipe_dots(SolverState* st, double g, double d) {
   st->c2 = d;
   if (1 < st->iter) {
     st->beta = g * gamma1;
-    st->alpha = g / (d - st->beta * g * alpha1);
+    // two roundings, left to right, as the reference's Fortran (no FMA)
+    st->alpha = g / __dsub_rn(d, __dmul_rn(__dmul_rn(st->beta, g), alpha1));
   } else {
     st->alpha = g / d;
     st->beta = 0.0;
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(kThreads)
   if (st->done) return;
   const bool init = st->iter == 0;
   if (!init && !st->rr_flag) return;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T y[B];
     sell_row<B, U, V, T>(A, x, row, y);
@@ -227,7 +228,7 @@ __global__ void __launch_bounds__(kThreads)
       const long long i = (long long)row * B + c;
       t[c] = sub_rn(b[i], y[c]);  // src/linalg/matvec.f90:902  R = 1.0*B + (-1.0)*R
       r[i] = t[c];
-      v[0] += (double)t[c] * (double)t[c];
+      v.add(0, t[c], t[c]);
     }
     if (mode != 1) {  // CG and PipeCG: z (PipeCG: U) = M^-1 r
       T w[B];
@@ -237,7 +238,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int c = 0; c < B; c++) {
         z[(long long)row * B + c] = w[c];
-        v[1] += (double)t[c] * (double)w[c];
+        v.add(1, t[c], w[c]);
       }
     } else {
 #pragma unroll
@@ -245,7 +246,7 @@ __global__ void __launch_bounds__(kThreads)
         const long long i = (long long)row * B + c;
         T rtv;
         if (init) { rt[i] = t[c]; rtv = t[c]; } else { rtv = rt[i]; }
-        v[1] += (double)t[c] * (double)rtv;
+        v.add(1, t[c], rtv);
       }
     }
   }
@@ -297,7 +298,7 @@ __global__ void __launch_bounds__(kThreads)
     cg_spmv_kernel(SellView<V> A, const T* __restrict__ p, T* __restrict__ q, double* partials,
                    unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
-  double v[1] = {0.0};
+  DotAcc<1, T> v;
   for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, p, row, y);
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < B; c++) {
       const long long i = (long long)row * B + c;
       q[i] = y[c];
-      v[0] += (double)p[i] * (double)y[c];
+      v.add(0, p[i], y[c]);
     }
   });
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
@@ -337,7 +338,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool alu_vec = (N % R) == 0;
   const long long ngroups = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) ? N / R : 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
     const long long row0 = g * R, e0 = row0 * B;
     T xv[E], pv[E];
@@ -369,8 +370,8 @@ __global__ void __launch_bounds__(kThreads)
       }
 #pragma unroll
       for (int i = 0; i < E; i++) {
-        v[0] += (double)rv[i] * (double)rv[i];
-        v[1] += (double)rv[i] * (double)zv[i];
+        v.add(0, rv[i], rv[i]);
+        v.add(1, rv[i], zv[i]);
       }
       vstore<T, E>(r + e0, rv);
       vstore<T, E>(z + e0, zv);
@@ -395,8 +396,8 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int c = 0; c < B; c++) {
         z[row * B + c] = w[c];
-        v[0] += (double)t[c] * (double)t[c];
-        v[1] += (double)t[c] * (double)w[c];
+        v.add(0, t[c], t[c]);
+        v.add(1, t[c], w[c]);
       }
     }
   }
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(kThreads)
                      T* __restrict__ mm, const T* __restrict__ alu, int prec, double* partials, unsigned int* ticket,
                      SolverState* st) {
   if (st->done) return;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) {
     T w[B];
 #pragma unroll
@@ -458,8 +459,8 @@ __global__ void __launch_bounds__(kThreads)
       const long long i = (long long)row * B + c;
       const T uv = u[i];
       w[c] = vv[i];
-      v[0] += (double)r[i] * (double)uv;
-      v[1] += (double)w[c] * (double)uv;
+      v.add(0, r[i], uv);
+      v.add(1, w[c], uv);
     }
     if (prec) diag_row<B, T>(alu, N, row, w);
 #pragma unroll
@@ -502,7 +503,7 @@ __global__ void __launch_bounds__(kThreads)
   if (st->done) return;
   const bool rr_iter = (st->iter % st->iter_rr) == 0;
   const T alpha = (T)st->alpha, beta = (T)st->beta;
-  double v[1] = {0.0};
+  DotAcc<1, T> v;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const T zi = add_rn(mul_rn(beta, z[i]), l[i]);
     const T qi = add_rn(mul_rn(beta, q[i]), mm[i]);
@@ -518,7 +519,7 @@ __global__ void __launch_bounds__(kThreads)
       r[i] = ri;
       u[i] = add_rn(mul_rn(-alpha, qi), u[i]);
       vv[i] = add_rn(mul_rn(-alpha, zi), vi);
-      v[0] += (double)ri * (double)ri;
+      v.add(0, ri, ri);
     }
     x[i] = add_rn(mul_rn(alpha, pi), x[i]);
   }
@@ -556,14 +557,14 @@ __global__ void __launch_bounds__(kThreads)
     grop_q_kernel(int N, const T* __restrict__ p, const T* __restrict__ s, T* __restrict__ q,
                   const T* __restrict__ alu, int prec, double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  double v[1] = {0.0};
+  DotAcc<1, T> v;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < N; row += gridDim.x * blockDim.x) {
     T w[B];
 #pragma unroll
     for (int c = 0; c < B; c++) {
       const long long i = (long long)row * B + c;
       w[c] = s[i];
-      v[0] += (double)p[i] * (double)w[c];
+      v.add(0, p[i], w[c]);
     }
     if (prec) diag_row<B, T>(alu, N, row, w);
 #pragma unroll
@@ -585,15 +586,15 @@ __global__ void __launch_bounds__(kThreads)
                        unsigned int* ticket, SolverState* st, double* hist) {
   if (st->done) return;
   const T alpha = (T)st->alpha;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     x[i] = add_rn(mul_rn(alpha, p[i]), x[i]);
     const T ri = add_rn(mul_rn(-alpha, s[i]), r[i]);
     const T ui = add_rn(mul_rn(-alpha, q[i]), u[i]);
     r[i] = ri;
     u[i] = ui;
-    v[0] += (double)ri * (double)ui;
-    v[1] += (double)ri * (double)ri;
+    v.add(0, ri, ui);
+    v.add(1, ri, ri);
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
     if (st->sharded) {
@@ -736,7 +737,7 @@ __global__ void __launch_bounds__(kThreads)
     bicg_v_kernel(SellView<V> A, const T* __restrict__ pt, T* __restrict__ vv, const T* __restrict__ rt,
                   double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
-  double v[1] = {0.0};
+  DotAcc<1, T> v;
   for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, pt, row, y);
@@ -744,7 +745,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < B; c++) {
       const long long i = (long long)row * B + c;
       vv[i] = y[c];
-      v[0] += (double)rt[i] * (double)y[c];
+      v.add(0, rt[i], y[c]);
     }
   });
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
@@ -803,7 +804,7 @@ __global__ void __launch_bounds__(kThreads)
     bicg_t_kernel(SellView<V> A, const T* __restrict__ stv, T* __restrict__ t, const T* __restrict__ s,
                   double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for_rows<kSet>(rs, A.N, [&](int row) {
     T y[B];
     sell_row<B, U, V, T>(A, stv, row, y);
@@ -811,8 +812,8 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < B; c++) {
       const long long i = (long long)row * B + c;
       t[i] = y[c];
-      v[0] += (double)y[c] * (double)s[i];
-      v[1] += (double)y[c] * (double)y[c];
+      v.add(0, y[c], s[i]);
+      v.add(1, y[c], y[c]);
     }
   });
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
@@ -844,7 +845,7 @@ __global__ void __launch_bounds__(kThreads)
   // x is the caller's vector: 16-byte accesses only when it is aligned
   const long long nv = ((reinterpret_cast<uintptr_t>(x) & 15) == 0) ? n / W : 0;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  double v[2] = {0.0, 0.0};
+  DotAcc<2, T> v;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nv; q += stride) {
     const long long i0 = q * W;
     T xv[W], ptv[W], sv_[W];
@@ -862,8 +863,8 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
       for (int k = 0; k < W; k++) {
         tv[k] = axpy_rn(-omega, tv[k], ssv[k]);
-        v[0] += (double)tv[k] * (double)tv[k];
-        v[1] += (double)tv[k] * (double)rtv[k];
+        v.add(0, tv[k], tv[k]);
+        v.add(1, tv[k], rtv[k]);
       }
       vstore<T, W>(r + i0, tv);
     }
@@ -873,8 +874,8 @@ __global__ void __launch_bounds__(kThreads)
     if (!rr_iter) {
       const T rv = axpy_rn(-omega, t[i], s[i]);
       r[i] = rv;
-      v[0] += (double)rv * (double)rv;
-      v[1] += (double)rv * (double)rt[i];
+      v.add(0, rv, rv);
+      v.add(1, rv, rt[i]);
     }
   }
   if (rr_iter) {
@@ -969,7 +970,7 @@ __global__ void __launch_bounds__(kThreads)
     mbicg_v_kernel(SellView2 A, const float* __restrict__ pt, float* __restrict__ vv, const float* __restrict__ rt,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  double v[1] = {0.0};
+  PlainAcc<1> v;
   const int npairs = (A.N + 1) / 2;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     float y0[B], y1[B];
@@ -983,7 +984,7 @@ __global__ void __launch_bounds__(kThreads)
         const long long i = (long long)(2 * t + h) * B + c;
         const float yv = h ? y1[c] : y0[c];
         vv[i] = yv;
-        v[0] += (double)rt[i] * (double)yv;
+        v.add(0, rt[i], yv);
       }
     }
   }
@@ -1001,7 +1002,7 @@ __global__ void __launch_bounds__(kThreads)
     mbicg_t_kernel(SellView2 A, const float* __restrict__ stv, float* __restrict__ t, const float* __restrict__ s,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  double v[2] = {0.0, 0.0};
+  PlainAcc<2> v;
   const int npairs = (A.N + 1) / 2;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < npairs; q += gridDim.x * blockDim.x) {
     float y0[B], y1[B];
@@ -1015,8 +1016,8 @@ __global__ void __launch_bounds__(kThreads)
         const long long i = (long long)(2 * q + h) * B + c;
         const float yv = h ? y1[c] : y0[c];
         t[i] = yv;
-        v[0] += (double)yv * (double)s[i];
-        v[1] += (double)yv * (double)yv;
+        v.add(0, yv, s[i]);
+        v.add(1, yv, yv);
       }
     }
   }
@@ -1083,7 +1084,7 @@ __global__ void __launch_bounds__(kThreads)
     cg_spmv2_kernel(SellView2 A, const float* __restrict__ p, float* __restrict__ q, double* partials,
                     unsigned int* ticket, SolverState* st) {
   if (st->done) return;
-  double v[1] = {0.0};
+  PlainAcc<1> v;
   const int npairs = (A.N + 1) / 2;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += gridDim.x * blockDim.x) {
     float y0[B], y1[B];
@@ -1092,14 +1093,14 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < B; c++) {
       const long long i = (long long)2 * t * B + c;
       q[i] = y0[c];
-      v[0] += (double)p[i] * (double)y0[c];
+      v.add(0, p[i], y0[c]);
     }
     if (2 * t + 1 < A.N) {
 #pragma unroll
       for (int c = 0; c < B; c++) {
         const long long i = (long long)(2 * t + 1) * B + c;
         q[i] = y1[c];
-        v[0] += (double)p[i] * (double)y1[c];
+        v.add(0, p[i], y1[c]);
       }
     }
   }
@@ -1125,7 +1126,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool alu_vec = (N % R) == 0;
   const long long ngroups = N / R;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  double v[2] = {0.0, 0.0};
+  PlainAcc<2> v;
   for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ngroups; g += stride) {
     const long long row0 = g * R, e0 = row0 * B;
     float yv[E], pv[E], rv[E], qv[E], zv[E];
@@ -1154,8 +1155,8 @@ __global__ void __launch_bounds__(kThreads)
     }
 #pragma unroll
     for (int i = 0; i < E; i++) {
-      v[0] += (double)rv[i] * (double)rv[i];
-      v[1] += (double)rv[i] * (double)zv[i];
+      v.add(0, rv[i], rv[i]);
+      v.add(1, rv[i], zv[i]);
     }
     vstore<float, E>(y + e0, yv);
     vstore<float, E>(r + e0, rv);
@@ -1175,8 +1176,8 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int c = 0; c < B; c++) {
       z[row * B + c] = w[c];
-      v[0] += (double)t[c] * (double)t[c];
-      v[1] += (double)t[c] * (double)w[c];
+      v.add(0, t[c], t[c]);
+      v.add(1, t[c], w[c]);
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_mixed_inner(st, tot[0], tot[1], hist); });
@@ -1204,7 +1205,7 @@ __global__ void __launch_bounds__(kThreads)
                          SolverState* st, double* hist, float* __restrict__ rt = nullptr) {
   if (st->done || !(st->iter == 0 || st->refresh)) return;
   const bool init = st->iter == 0;
-  double v[2] = {0.0, 0.0};
+  PlainAcc<2> v;
   const XPlusY xy{x, y};
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     // (A (x + y))[row] in FP64, blocks in CSR order, U slots in flight
@@ -1215,7 +1216,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int c = 0; c < B; c++) {
       const long long i = (long long)row * B + c;
       const double rv = b[i] - ax[c];
-      v[0] += rv * rv;
+      v.s[0] += rv * rv;
       t[c] = (float)rv;
       r[i] = t[c];
       w[c] = t[c];
@@ -1226,14 +1227,14 @@ __global__ void __launch_bounds__(kThreads)
         const long long i = (long long)row * B + c;
         float rtv;
         if (init) { rt[i] = t[c]; rtv = t[c]; } else { rtv = rt[i]; }
-        v[1] += (double)t[c] * (double)rtv;
+        v.add(1, t[c], rtv);
       }
     } else {
       if (prec) diag_row<B, float>(alu, A.N, row, w);
 #pragma unroll
       for (int c = 0; c < B; c++) {
         z[(long long)row * B + c] = w[c];
-        v[1] += (double)t[c] * (double)w[c];
+        v.add(1, t[c], w[c]);
       }
     }
   }

@@ -11,6 +11,14 @@ Runs the CPU oracle (oracle/_build/libmonolis_oracle.so); long at full size
 summation orders of every dot product) and stores the counts under
 "<key>:by_threads": how far the iteration count moves when only the
 summation order changes.
+
+--dot-mode n128 runs the oracle with every dot product summed in
+double-double (the arithmetic of the reference's pseudo-quadruple inner
+product, src/linalg/inner_product.f90:219-258, which the product library's
+FP64 kernels use) and stores the results under "<key>:n128...": the
+iteration count, the thread counts it was reproduced with (--spread), and
+a strided sample of the solution ("<key>:n128:x_sample", every
+--sample-stride-th entry, first entry at 0).
 """
 import argparse
 import json
@@ -46,9 +54,14 @@ def main():
     ap.add_argument("--threads", type=int, default=os.cpu_count())
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--spread", action="store_true")
+    ap.add_argument("--dot-mode", choices=("reference", "n128"), default="reference")
+    ap.add_argument("--sample-stride", type=int, default=0)
     args = ap.parse_args()
     lib = api.load_library(SO, oracle=True)
     lib.oracle_set_threads(args.threads)
+    n128 = args.dot_mode == "n128"
+    lib.oracle_set_dot_mode(1 if n128 else 0)
+    sfx = ":n128" if n128 else ""
     data = {}
     if os.path.exists(OUT):
         with open(OUT) as f:
@@ -75,7 +88,7 @@ def main():
                 counts[str(th)] = m.get_converge_iter()
                 m.finalize()
                 print(key, th, counts[str(th)], flush=True)
-            data[key + ":by_threads"] = counts
+            data[key + sfx + ":by_threads"] = counts
             with open(OUT, "w") as f:
                 json.dump(data, f, indent=1, sort_keys=True)
             continue
@@ -93,12 +106,17 @@ def main():
         t0 = time.time()
         m.solve(b, x)
         dt = time.time() - t0
-        data[key] = m.get_converge_iter()
-        data[key + ":residual"] = m.get_converge_residual()
-        data[key + ":status"] = m.get_error_tag()
-        data[key + ":threads"] = args.threads
-        data[key + ":seconds"] = round(dt, 1)
-        print(key, data[key], data[key + ":residual"], f"{dt:.0f}s", flush=True)
+        k = key + sfx
+        data[k] = m.get_converge_iter()
+        data[k + ":residual"] = m.get_converge_residual()
+        data[k + ":status"] = m.get_error_tag()
+        data[k + ":threads"] = args.threads
+        data[k + ":seconds"] = round(dt, 1)
+        if args.sample_stride > 0:
+            data[k + ":x_stride"] = args.sample_stride
+            data[k + ":x_sample"] = [float(v) for v in x[::args.sample_stride]]
+            data[k + ":x_norm"] = float(np.linalg.norm(x))
+        print(k, data[k], data[k + ":residual"], f"{dt:.0f}s", flush=True)
         m.finalize()
         with open(OUT, "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)

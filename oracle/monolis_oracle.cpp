@@ -52,6 +52,13 @@ double now_sec() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
+// Optional wall-clock log of a solve (CPU baseline timing): entry 0 at the
+// start of monolis_solve_R, entry i at the end of iteration i (its
+// convergence check). Set by oracle_set_iter_clock; the arithmetic is not
+// touched.
+double* g_iter_clock = nullptr;
+int g_iter_clock_cap = 0;
+
 template <class T>
 T* alloc_zero(long long n) {
   if (n <= 0) n = 1;
@@ -257,8 +264,75 @@ void matvec(const MONOLIS_MAT* a, int N, const double* X, double* Y) {
   }
 }
 
+// Error-free addition (Knuth's TwoSum): s + e == a + b exactly.
+inline void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+inline void dd_add(double& hi, double& lo, double p) {
+  double s, e;
+  two_sum(hi, p, s, e);
+  e = e + lo;
+  hi = s + e;
+  lo = e - (hi - s);
+}
+inline void dd_merge(double& hi, double& lo, double h2, double l2) {
+  double s, e;
+  two_sum(hi, h2, s, e);
+  e = e + (lo + l2);
+  hi = s + e;
+  lo = e - (hi - s);
+}
+
+// Sum of the rounded products X(i)*Y(i) in double-double, the arithmetic of
+// the reference's pseudo-quadruple inner product
+// (src/linalg/inner_product.f90:219-258: each product rounded to double,
+// added to a two-double sum, the sum converted back to double). Each thread
+// sums a contiguous chunk, every addition a double-double addition
+// renormalised after each step (Dekker 1971), and the chunks are combined in
+// thread order the same way; the result is within a small multiple of
+// n eps^2 sum|x_i y_i| of the exact sum of the rounded products, so it does
+// not depend on the thread count (nor on any other grouping) except in the
+// rare case of an exact sum that close to a rounding boundary. The
+// monolis_utils routine the reference calls for the two-double addition
+// (monolis_add_R_N128) is not in the reference tree; this is the standard
+// TwoSum-based addition.
+double dot_n128(long long m, const double* X, const double* Y) {
+#ifdef _OPENMP
+  const int nt = omp_get_max_threads();
+#else
+  const int nt = 1;
+#endif
+  std::vector<double> H(nt, 0.0), L(nt, 0.0);
+  int used = 1;
+#pragma omp parallel
+  {
+#ifdef _OPENMP
+    const int t = omp_get_thread_num(), T = omp_get_num_threads();
+#else
+    const int t = 0, T = 1;
+#endif
+    if (t == 0) used = T;
+    const long long i0 = m * t / T, i1 = m * (t + 1) / T;
+    double hi = 0.0, lo = 0.0;
+    for (long long i = i0; i < i1; i++) dd_add(hi, lo, X[i] * Y[i]);
+    H[t] = hi;
+    L[t] = lo;
+  }
+  double hi = 0.0, lo = 0.0;
+  for (int t = 0; t < used; t++) dd_merge(hi, lo, H[t], L[t]);
+  return hi + lo;
+}
+
+// Dot products of the solvers and of monolis_inner_product_R: 0 = the
+// reference's inner product (below); 1 = every dot product in double-double
+// (dot_n128), the arithmetic the product library's FP64 kernels use.
+int g_dot_mode = 0;
+
 // src/linalg/inner_product.f90:148-190 (allreduce is the identity on one rank)
 double dot(long long m, const double* X, const double* Y) {
+  if (g_dot_mode == 1) return dot_n128(m, X, Y);
   double sum = 0.0;
 #pragma omp parallel for reduction(+ : sum) schedule(static)
   for (long long i = 0; i < m; i++) sum = sum + X[i] * Y[i];
@@ -376,6 +450,7 @@ bool check_converge(MONOLIS_PRM* prm, long long nndof, const double* R, double B
   double R2 = dot(nndof, R, R);
   t.dotp += now_sec() - t1;
   double resid = std::sqrt(R2 / B2);
+  if (g_iter_clock && iter < g_iter_clock_cap) g_iter_clock[iter] = now_sec();
   prm->Iarray[MONOLIS_PRM_I_CUR_ITER] = iter;
   prm->Rarray[MONOLIS_PRM_R_CUR_RESID] = resid;
   if (prm->Iarray[MONOLIS_PRM_I_SHOW_ITERLOG] == MONOLIS_I_TRUE) printf("%7d%16.6E\n", iter, resid);
@@ -438,8 +513,12 @@ int solver_CG(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
   return status ? status : 1;
 }
 
-// src/iterative/BiCGSTAB.f90:18-192
-int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t) {
+// src/iterative/BiCGSTAB.f90:18-192; with n128, src/iterative/
+// BiCGSTAB_N128.f90:18-153, which takes rho = <R,RT> and c2 = <RT,V> in
+// double-double (:73, :90) and everything else as BiCGSTAB.f90 (its
+// (T,S), (T,T) pass through a double-double all-reduce, the identity at
+// one rank, :104-108).
+int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t, bool n128 = false) {
   double* X = a->R.X;
   const double* B = a->R.B;
   const int iter_RR = g_iter_rr;
@@ -459,7 +538,7 @@ int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t)
   int status = 0;
   for (int iter = 1; iter <= prm->Iarray[MONOLIS_PRM_I_MAX_ITER]; iter++) {
     double t1 = now_sec();
-    rho = dot(nndof, R.data(), RT.data());
+    rho = n128 ? dot_n128(nndof, R.data(), RT.data()) : dot(nndof, R.data(), RT.data());
     if (std::fabs(rho) == 0.0) rho = sorted_dot(nndof, R.data(), RT.data());
     t.dotp += now_sec() - t1;
     if (1 < iter) {
@@ -476,7 +555,7 @@ int solver_BiCGSTAB(MONOLIS_PRM* prm, MONOLIS_MAT* a, const Prec& pc, Timers& t)
     matvec(a, a->N, PT.data(), V.data());
     t.spmv += now_sec() - t1;
     t1 = now_sec();
-    c2 = dot(nndof, RT.data(), V.data());
+    c2 = n128 ? dot_n128(nndof, RT.data(), V.data()) : dot(nndof, RT.data(), V.data());
     if (std::fabs(c2) == 0.0) c2 = sorted_dot(nndof, RT.data(), V.data());
     t.dotp += now_sec() - t1;
     alpha = rho / c2;
@@ -664,6 +743,7 @@ void solve_main(MONOLIS_PRM* prm, MONOLIS_MAT* a) {
   int status;
   if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_CG) status = solver_CG(prm, a, pc, t);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_BICGSTAB) status = solver_BiCGSTAB(prm, a, pc, t);
+  else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_BICGSTAB_N128) status = solver_BiCGSTAB(prm, a, pc, t, true);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_PIPECG) status = solver_PipeCG(prm, a, pc, t);
   else if (I[MONOLIS_PRM_I_METHOD] == MONOLIS_ITER_GROPCG) status = solver_GropCG(prm, a, pc, t);
   else error_stop("please select a linear solver for real numbers");
@@ -943,6 +1023,7 @@ void monolis_inner_product_R(MONOLIS* m, MONOLIS_COM* com, int n_dof, double* x,
 // src/solver/solver.f90:29-49: copy B and X in, solve, copy X out.
 void monolis_solve_R(MONOLIS* m, MONOLIS_COM* com, double* b, double* x) {
   (void)com;
+  if (g_iter_clock && g_iter_clock_cap > 0) g_iter_clock[0] = now_sec();
   MONOLIS_MAT* a = &m->mat;
   long long npndof = (long long)a->NP * a->NDOF;
   for (long long i = 0; i < npndof; i++) a->R.B[i] = b[i];
@@ -960,6 +1041,12 @@ void oracle_set_threads(int n) {
 #else
   (void)n;
 #endif
+}
+// Wall-clock log of the following solves (see g_iter_clock); buf = NULL
+// switches it off.
+void oracle_set_iter_clock(double* buf, int cap) {
+  g_iter_clock = buf;
+  g_iter_clock_cap = buf ? cap : 0;
 }
 void oracle_set_iter_rr(int n) {
   g_iter_rr = n > 0 ? n : 200;
@@ -1009,6 +1096,11 @@ void oracle_diag_apply(MONOLIS* m, const double* ALU, const double* x, double* y
   diag_apply(&m->mat, v, x, y);
 }
 double oracle_dot(long long n, const double* x, const double* y) { return dot(n, x, y); }
+double oracle_dot_n128(long long n, const double* x, const double* y) { return dot_n128(n, x, y); }
+// 0: the reference's inner product in every solver and in monolis_inner_product_R;
+// 1: double-double (dot_n128) everywhere.
+void oracle_set_dot_mode(int mode) { g_dot_mode = mode == 1 ? 1 : 0; }
+int oracle_get_dot_mode(void) { return g_dot_mode; }
 double oracle_sorted_dot(long long n, const double* x, const double* y) { return sorted_dot(n, x, y); }
 
 // check_converge restated for the known-answer test of mat_converge_test.f90.

@@ -1,4 +1,6 @@
 """Shared helpers: build a problem in a library, solve it, compare."""
+import contextlib
+
 import numpy as np
 
 from monolis_b200 import api
@@ -43,3 +45,15 @@ def bits_equal(a, b):
     a = np.ascontiguousarray(a, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
     return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+@contextlib.contextmanager
+def oracle_dot_mode(oracle, mode):
+    """Runs the oracle with its dot products in the given arithmetic: 0 the
+    reference's plain sums, 1 double-double (the product's FP64 kernels)."""
+    old = oracle.oracle_get_dot_mode()
+    oracle.oracle_set_dot_mode(mode)
+    try:
+        yield
+    finally:
+        oracle.oracle_set_dot_mode(old)

@@ -344,3 +344,26 @@ def test_partition_tables_are_consistent():
             send_glob = ps["glob"][ps["send_item"][ps["send_index"][k]:ps["send_index"][k + 1]]]
             assert np.array_equal(recv_glob, send_glob)
         assert np.all(p["item"] < p["NP"])
+
+
+@pytest.mark.parametrize("problem,nd,world", [("laplacian", 1, 4), ("laplacian", 1, 3), ("elasticity", 3, 2),
+                                              ("elasticity", 3, 5)])
+def test_partition_rank_matches_partition_rows(problem, nd, world):
+    """The vectorised one-rank partitioner (used for the 56 M-block headline
+    system) gives exactly the arrays of the row-by-row one for every rank."""
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    from monolis_b200 import partition
+    m, b = global_system(problem)
+    args = (m.csr_index(), m.csr_item() - 1, m.values(), nd, world)
+    parts = partition.partition_rows(*args)
+    for r in range(world):
+        q = partition.partition_rank(*args, r)
+        p = parts[r]
+        for k in ("N", "NP", "lo", "hi"):
+            assert p[k] == q[k], k
+        for k in ("glob", "index", "item", "val", "recv_pe", "recv_index", "recv_item", "send_pe", "send_index",
+                  "send_item"):
+            assert np.array_equal(np.asarray(p[k]), np.asarray(q[k])), k
+            if k != "val" and k != "glob":
+                assert np.asarray(q[k]).dtype == np.int32, k

@@ -87,3 +87,50 @@ def test_multi_rhs_zero_and_maxiter(gpu, oracle):
     mp.set_tolerance(1e-14)
     X, its, res, st = mp.solve_multi(B)
     assert st[0] == 1 and st[2] == 1 and st[1] == 0 and its[0] == 4
+
+
+def test_multi_barrier_wait_runs_out(gpu):
+    """Every grid-barrier wait of the persistent kernel is bounded. With the
+    bound at 2,000 polls and block 0 reaching the first barrier 20 ms late
+    (MONOLIS_B200_PRM_I_WAIT_DELAY_US, a bounded sleep), the other blocks'
+    waits run out: the solve returns MONOLIS_B200_TIMEOUT (4) after every
+    block has left the kernel, and the next solve on the same device and
+    buffers (default bound, no delay) succeeds."""
+    m = product_fv(gpu, 12, 77, precision=1)
+    B = np.stack([P.uniform(900 + k, 12 ** 3) for k in range(3)])
+    m.Iarray[api.B200_PRM_I_WAIT_LIMIT] = 2000
+    m.Iarray[api.B200_PRM_I_WAIT_DELAY_US] = 20000
+    with pytest.raises(RuntimeError, match="timeout"):
+        m.solve_multi(B)
+    assert m.Iarray[api.PRM_I_IERR] == 4
+    m.Iarray[api.B200_PRM_I_WAIT_LIMIT] = 0
+    m.Iarray[api.B200_PRM_I_WAIT_DELAY_US] = 0
+    X, its, res, st = m.solve_multi(B)
+    assert np.all(st == 0) and np.all(res < 1e-8)
+    ix, it, v, _ = P.fv_diffusion_csr(12, 77)
+    for k in range(3):
+        assert np.linalg.norm(B[k] - P.csr_matvec(ix, it, v, X[k])) / np.linalg.norm(B[k]) < 1.01e-8
+
+
+def test_multi_repeated_solve_reuses_its_graph(gpu):
+    """The chunk's launch sequence is a captured CUDA graph; solving again
+    with the same device buffers relaunches it and gives the same bits."""
+    import torch
+    m = product_fv(gpu, 14, 78, precision=0)
+    m.set_matrix_cache(True)
+    m.device_prepare()
+    K, n = 5, 14 ** 3
+    d_B = torch.from_numpy(np.stack([P.uniform(950 + k, n) for k in range(K)])).cuda()
+    outs = []
+    d_X = torch.zeros_like(d_B)
+    for _ in range(2):
+        d_X.zero_()
+        its = np.zeros(K, dtype=np.int32)
+        res = np.zeros(K)
+        st = np.zeros(K, dtype=np.int32)
+        rc = gpu.monolis_b200_device_solve_multi_R(m.p, K, d_B.data_ptr(), d_X.data_ptr(), its.ctypes.data_as(api._ip),
+                                                   res.ctypes.data_as(api._dp), st.ctypes.data_as(api._ip))
+        assert rc == 0 and np.all(st == 0)
+        outs.append((d_X.cpu().numpy(), its.copy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])

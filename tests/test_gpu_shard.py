@@ -121,3 +121,45 @@ def test_sharded_boundary_rows_through_self_halo(gpu, problem, kw, method):
     assert abs(its - it_ref) <= 2, (its, it_ref)
     assert np.linalg.norm(xs[:N * nd] - x_ref) / np.linalg.norm(x_ref) < 1e-9
     ms.finalize()
+
+
+@pytest.mark.parametrize("problem,kw,method", [
+    ("elasticity", dict(n=10), api.ITER_CG),
+    ("convection_diffusion", dict(n=16, peclet=5.0), api.ITER_BICGSTAB),
+])
+def test_device_solve_com_one_rank(gpu, problem, kw, method):
+    """monolis_b200_device_solve_com_R (device b and x, multi-rank plan through
+    a one-rank NCCL communicator) gives the bits of the plain device solve;
+    without a communicator it is the plain device solve."""
+    import torch
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    mp.set_method(method)
+    mp.set_precond(api.PREC_DIAG)
+    mp.set_tolerance(1e-8)
+    mp.set_matrix_cache(True)
+    mp.device_prepare()
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    assert mp.device_solve(d_b.data_ptr(), d_x.data_ptr()) == 0
+    x_ref, it_ref = d_x.cpu().numpy(), mp.get_converge_iter()
+    d_x.zero_()
+    assert mp.device_solve_com(d_b.data_ptr(), d_x.data_ptr()) == 0  # no communicator attached
+    assert bits_equal(d_x.cpu().numpy(), x_ref)
+    p = partition.partition_rank(mp.csr_index(), mp.csr_item() - 1, mp.values(), nd, 1, 0)
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(p["N"], p["NP"], nd, len(p["item"]), p["val"], p["index"], p["item"])
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_method(method)
+    ms.set_precond(api.PREC_DIAG)
+    ms.set_tolerance(1e-8)
+    ms.set_matrix_cache(True)
+    ms.set_halo(p, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    ms.device_prepare()
+    d_x2 = torch.zeros_like(d_b)
+    assert ms.device_solve_com(d_b.data_ptr(), d_x2.data_ptr()) == 0
+    assert ms.get_converge_iter() == it_ref
+    assert bits_equal(d_x2.cpu().numpy(), x_ref)
+    ms.finalize()

@@ -37,10 +37,10 @@ def chain(lib, n_dof, rng, diag_shift=2.0):
 @pytest.mark.parametrize("n_dof", [1, 2, 3])
 @pytest.mark.parametrize("prec", [api.PREC_NONE, api.PREC_DIAG])
 @pytest.mark.parametrize("method,tol", [(api.ITER_CG, 1e-10), (api.ITER_BICGSTAB, 1e-12), (api.ITER_PIPECG, 1e-10),
-                                        (api.ITER_GROPCG, 1e-10)])
+                                        (api.ITER_GROPCG, 1e-10), (api.ITER_BICGSTAB_N128, 1e-12)])
 def test_chain_solve_x_equals_one(oracle, n_dof, prec, method, tol):
     # src_test/iterative/CG_test.f90:74-89, BiCGSTAB_test.f90 (tol 1e-12), PipeCG_test.f90:74-89,
-    # GropCG_test.f90
+    # GropCG_test.f90, BiCGSTAB_N128_test.f90 (tol 1e-12)
     m = chain(oracle, n_dof, np.random.default_rng(10 * n_dof + prec))
     m.quiet()
     b = m.matvec(np.ones(10 * n_dof))
@@ -210,3 +210,55 @@ def test_zero_rhs_gives_zero(oracle):
     x = np.ones(10)
     m.solve(np.zeros(10), x)
     assert np.all(x == 0.0)
+
+
+def test_inner_product_n128(oracle):
+    # src_test/linalg/inner_product_test.f90:146-158 (case 8): the
+    # pseudo-quadruple inner product of (1,1,1,1) and (1,2,3,4) is 10
+    dp = C.POINTER(C.c_double)
+    x, y = np.ones(4), np.array([1.0, 2.0, 3.0, 4.0])
+    assert oracle.oracle_dot_n128(4, x.ctypes.data_as(dp), y.ctypes.data_as(dp)) == 10.0
+    # the two-double sum keeps what a double sum absorbs
+    x = np.array([1e16, 1.0, -1e16, 1.0])
+    assert oracle.oracle_dot_n128(4, x.ctypes.data_as(dp), np.ones(4).ctypes.data_as(dp)) == 2.0
+
+
+@pytest.mark.parametrize("n", [1, 17, 100_003, 2_000_000])
+def test_inner_product_n128_is_the_rounded_exact_sum(oracle, n):
+    """The double-double sum of the rounded products equals the correctly
+    rounded exact sum of those products (math.fsum) for 1 to 8 threads: its
+    value does not depend on the summation order."""
+    import math
+    dp = C.POINTER(C.c_double)
+    rng = np.random.default_rng(n)
+    x, y = rng.standard_normal(n), rng.standard_normal(n)
+    exact = math.fsum((x * y).tolist())
+    try:
+        for th in (1, 2, 3, 8):
+            oracle.oracle_set_threads(th)
+            assert oracle.oracle_dot_n128(n, x.ctypes.data_as(dp), y.ctypes.data_as(dp)) == exact
+    finally:
+        oracle.oracle_set_threads(1)
+
+
+def test_dot_mode_n128_makes_bicgstab_order_free(oracle):
+    """With every dot product in double-double, BiCGSTAB on a 48^3
+    convection-diffusion system gives bit-identical solutions and the same
+    iteration count for 1, 2, 4 and 8 threads (the reference's plain sums
+    are order-dependent: the same runs give different bits)."""
+    from helpers import build
+    outs = {}
+    try:
+        oracle.oracle_set_dot_mode(1)
+        for th in (1, 2, 4, 8):
+            oracle.oracle_set_threads(th)
+            m, b = build(oracle, "convection_diffusion", n=48, peclet=50.0)
+            x, it, res, st = solve(m, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=1e-8)
+            assert st == 0
+            outs[th] = (it, x)
+    finally:
+        oracle.oracle_set_dot_mode(0)
+        oracle.oracle_set_threads(1)
+    it1, x1 = outs[1]
+    for it, x in outs.values():
+        assert it == it1 and bits_equal(x, x1)

@@ -1,5 +1,6 @@
 """The allocation-free inner product (monolis_b200_inner_product_noalloc_R)
-against the library's regular inner product (monolis_inner_product_R).
+against an independent host sum (math.fsum of the exact products) and the
+library's regular inner product (monolis_inner_product_R).
 
 The no-alloc entry point is for callers that cannot call cudaMalloc when they
 need a dot product (an application that keeps all device memory in its own
@@ -8,6 +9,8 @@ reduction scratch is a fixed array inside the library. This file is named so
 that pytest collects it last; it also passes on its own in a fresh process.
 """
 import ctypes as C
+import math
+from fractions import Fraction
 
 import numpy as np
 import pytest
@@ -31,27 +34,65 @@ def _regular_dot(lib, x, y):
     return s
 
 
+def _exact_dot(x, y):
+    """The dot product rounded once: each product taken exactly (a rational
+    number), split into two doubles (its rounding and the remainder, which
+    is exact: a product of two doubles has at most 106 significant bits),
+    and all of them summed exactly by math.fsum."""
+    terms = []
+    for a, b in zip(x.tolist(), y.tolist()):
+        p = Fraction(a) * Fraction(b)
+        hi = float(p)
+        terms.append(hi)
+        terms.append(float(p - Fraction(hi)))
+    return math.fsum(terms)
+
+
+def _noalloc(lib, n, d_x, d_y, stream):
+    import torch
+
+    d_out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    rc = lib.monolis_b200_inner_product_noalloc_R(n, C.c_void_p(d_x.data_ptr()), C.c_void_p(d_y.data_ptr()),
+                                                 C.c_void_p(d_out.data_ptr()), C.c_void_p(stream.cuda_stream))
+    assert rc == 0
+    stream.synchronize()
+    return d_out.item()
+
+
 def test_noalloc_inner_product_matches_regular(gpu):
     import torch
 
     lib = gpu
     stream = torch.cuda.current_stream()
     rng = np.random.default_rng(2024)
-    n = 1_000_003
+    n = 200_003
     for call in range(2):  # two calls in a row share the same device scratch
         x = rng.standard_normal(n)
         y = rng.standard_normal(n) + (0.5 if call else 0.0)
+        exact = _exact_dot(x, y)
         ref = _regular_dot(lib, x, y)
-        d_x = torch.from_numpy(x).cuda()
-        d_y = torch.from_numpy(y).cuda()
-        d_out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
-        rc = lib.monolis_b200_inner_product_noalloc_R(n, C.c_void_p(d_x.data_ptr()), C.c_void_p(d_y.data_ptr()),
-                                                     C.c_void_p(d_out.data_ptr()), C.c_void_p(stream.cuda_stream))
-        assert rc == 0
-        stream.synchronize()
-        got = d_out.item()
-        # the two kernels sum in different orders: relative 1e-13 of sum |x_i y_i|
-        assert abs(got - ref) <= 1e-13 * float(np.abs(x * y).sum()), (call, got, ref)
+        got = _noalloc(lib, n, torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), stream)
+        # a tree of FP64 sums: within 1e-13 of sum |x_i y_i| of the exact value
+        scale = float(np.abs(x * y).sum())
+        assert abs(got - exact) <= 1e-13 * scale, (call, got, exact)
+        assert abs(got - ref) <= 1e-13 * scale, (call, got, ref)
+
+
+def test_noalloc_empty_and_full_capacity(gpu):
+    """n = 0 gives 0 (the result is still written); n at the stated maximum
+    runs, checked against a numpy sum of the same products."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+    d = torch.ones(1, dtype=torch.float64, device="cuda")
+    assert _noalloc(gpu, 0, d, d, stream) == 0.0
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(MAX_N)
+    y = rng.standard_normal(MAX_N)
+    ref = float(np.dot(x, y))
+    for _ in range(2):
+        got = _noalloc(gpu, MAX_N, torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), stream)
+        assert abs(got - ref) <= 1e-12 * float(np.abs(x * y).sum()), (got, ref)
 
 
 def test_noalloc_rejects_oversize(gpu):
