@@ -209,11 +209,13 @@ def workload_c3(lib, args, peak):
             m.set_precision(prec)
             m.device_prepare()
             device_solve_timed(m, stream, d_b, d_x)  # warm-up
-            t = device_solve_timed(m, stream, d_b, d_x)
+            with ClockSampler(torch.cuda.current_device()) as clk:
+                ts = [device_solve_timed(m, stream, d_b, d_x) for _ in range(3)]
+            t = float(np.mean(ts))
             d_r = torch.empty_like(d_x)
             m.device_matvec(d_x.data_ptr(), d_r.data_ptr())
             stream.synchronize()
-            res[name] = {"s": t, "iterations": m.get_converge_iter(),
+            res[name] = {"s": t, "s_each": ts, "clocks": clk.summary(), "iterations": m.get_converge_iter(),
                          "true_rel_residual": (torch.linalg.norm(d_b - d_r) / torch.linalg.norm(d_b)).item(),
                          "fp64_refreshes": int(m.Iarray[api.B200_PRM_I_N_REFINE])}
             if prec == 0:
@@ -332,9 +334,17 @@ def batch_run(lib, systems, bs, label):
         t_dev = batch.last_seconds()
         true = [float(np.linalg.norm(b - problems.csr_matvec(ix, it, v, x)) / np.linalg.norm(b))
                 for (ix, it, v, _), x, b in zip(systems, xs, bs)]
+        # roofline: every system's iterations x the minimum fused FP32 CG schedule of its size (SpMV:
+        # values and 32-bit column ids, offsets, x and y; 12 vector passes; DIAG factors), FP64 refreshes
+        # not counted (a lower bound on the bytes of the refined solve)
+        peak, _ = measured_peak()
+        byts = sum(int(k) * (len(it) * 8 + (len(ix) + 1) * 4 + 2 * (len(ix) - 1) * 4 + 13 * (len(ix) - 1) * 4)
+                   for k, (ix, it, v, _) in zip(its2, systems))
         out[name] = {"s": t_dev, "e2e_s": t_e2e, "all_converged": bool(np.all(st2 == 0)),
                      "max_true_rel_residual": max(true), "iterations_max": int(its2.max()),
-                     "iterations_mean": float(its2.mean())}
+                     "iterations_mean": float(its2.mean()),
+                     "roofline": {"bound": "hbm", "fp32_loop_bytes": float(byts),
+                                  "achieved_gbs": byts / t_dev / 1e9, "frac_of_measured": byts / t_dev / 1e9 / peak}}
     batch.destroy()
     log(f"[rank 0] batch {label}: {json.dumps({k: out[k] for k in out if k != 'autotune'})[:300]}")
     return out
@@ -456,8 +466,16 @@ def multi_rhs_run(lib, sysm, rhs):
         X = d_X.cpu().numpy()
         true = [float(np.linalg.norm(b - problems.csr_matvec(ix, it, v, X[k])) / np.linalg.norm(b))
                 for k, b in enumerate(rhs)]
+        # roofline: per iteration the matrix once (values + 32-bit column ids + offsets, in the loop
+        # precision) while any right-hand side is active, and 12 vector passes plus the DIAG factors
+        # per active right-hand side; FP64 refreshes not counted
+        peak, _ = measured_peak()
+        sv = 4 if prec == 1 else 8
+        byts = int(its.max()) * (len(it) * (sv + 4) + (n + 1) * 4) + float(its.sum()) * 13 * n * sv
         out[name] = {"s": times[-1], "all_converged": bool(np.all(st == 0)), "max_true_rel_residual": max(true),
-                     "iterations_max": int(its.max()), "iterations_mean": float(its.mean())}
+                     "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
+                     "roofline": {"bound": "hbm", "loop_bytes": float(byts), "achieved_gbs": byts / times[-1] / 1e9,
+                                  "frac_of_measured": byts / times[-1] / 1e9 / peak}}
     m.finalize()
     log(f"[rank 0] many rhs: {json.dumps(out)[:300]}")
     return out
@@ -530,37 +548,80 @@ def workload_c5(lib, args):
                      "total_s": t_fwd + t_adj + t_grad}
         if prec == 0:
             x_ref = d_x.cpu().numpy()
+            # roofline: the minimum fused CG schedule per iteration (SpMV + 12 vector passes + the
+            # DIAG factors, ndof 1) x iterations / solve time; the gradient kernel's bytes / its time
+            peak, peak_kind = measured_peak()
+            nn = n ** 3
+            it_bytes = float(m.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64]) + 12 * nn * 8 + nn * 8
+            c5_roofline = {"bound": "hbm", "peak_gbs": peak, "peak_kind": peak_kind,
+                           "cg_bytes_per_iteration": it_bytes,
+                           "fp64_forward_frac": it_f * it_bytes / t_fwd / 1e9 / peak,
+                           "fp64_adjoint_frac": it_a * it_bytes / t_adj / 1e9 / peak,
+                           "gradient_kernel_bytes": gbytes,
+                           "gradient_kernel_frac": gbytes / t_grad / 1e9 / peak}
     g64 = grads["fp64"]
     res["mixed"]["gradient_rel_diff_vs_fp64"] = float(np.linalg.norm(grads["mixed"] - g64) / np.linalg.norm(g64))
     fd = []
+    t_fd = 0.0
     if args.c5_fd_dirs > 0:
-        # central differences through the public API: assemble A(kappa +- h d) on the host, solve on the GPU
+        # central differences: A(kappa +- h d) assembled on the device (element matrices scaled per element,
+        # Dirichlet face), solved to 1e-11 on the device, loss summed on the device
+        import ctypes as C
         rng = np.random.default_rng(2025)
         h = 1e-4
+        fm = api.Monolis(lib)
+        fm.get_nonzero_pattern_flat(n ** 3, 8, 1, elem)
+        fm.quiet()
+        fm.set_error_abort(False)
+        fm.set_method(api.ITER_CG)
+        fm.set_precond(api.PREC_DIAG)
+        fm.set_tolerance(1e-11)
+        fm.set_maxiter(20000)
+        nodes = np.arange(0, n ** 3, n, dtype=np.int32)
+        zeros = np.zeros(len(nodes), dtype=np.int32)
+        vals = np.zeros(len(nodes))
+        ones = torch.ones(n ** 3, dtype=torch.float64, device="cuda")
+        d_fb = torch.empty_like(ones)
+        d_fx = torch.empty_like(ones)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
 
-        def loss(kap):
-            mm = api.Monolis(lib)
-            bb, _, _, _ = problems.diffusion_kappa(mm, n=n, kappa=kap)
-            mm.quiet()
-            mm.set_error_abort(False)
-            mm.set_method(api.ITER_CG)
-            mm.set_precond(api.PREC_DIAG)
-            mm.set_tolerance(1e-12)
-            mm.set_maxiter(50000)
-            xx = np.zeros_like(bb)
-            mm.solve(bb, xx)
-            mm.finalize()
-            return 0.5 * float(np.dot(xx - target, xx - target))
+        def loss(d_kap):
+            d_fb.copy_(ones)
+            rc = lib.monolis_b200_device_clear_matrix(fm.p)
+            rc = rc or lib.monolis_b200_device_add_elements_R(fm.p, n_elem, 8, d_elem.data_ptr(), d_k.data_ptr(), 0,
+                                                              d_kap.data_ptr())
+            rc = rc or lib.monolis_b200_device_set_Dirichlet_bc_R(fm.p, d_fb.data_ptr(), len(nodes),
+                                                                  nodes.ctypes.data_as(ip), zeros.ctypes.data_as(ip),
+                                                                  vals.ctypes.data_as(dp))
+            if rc:
+                raise RuntimeError(f"FD assembly failed: {rc}")
+            d_fx.zero_()
+            rc = fm.device_solve(d_fb.data_ptr(), d_fx.data_ptr())
+            fd_solves.append((int(rc), fm.get_converge_iter(), fm.get_converge_residual()))
+            return 0.5 * float(torch.dot(d_fx - d_t, d_fx - d_t))
+        fd_solves = []
+        d_kap0 = torch.from_numpy(kappa).cuda()
+        g64_d = torch.from_numpy(g64).cuda()
+        t0 = time.perf_counter()
         for _ in range(args.c5_fd_dirs):
-            d = kappa * rng.standard_normal(n_elem)
-            fdv = (loss(kappa + h * d) - loss(kappa - h * d)) / (2 * h)
-            an = float(np.dot(g64, d))
+            d = torch.from_numpy(kappa * rng.standard_normal(n_elem)).cuda()
+            fdv = (loss(d_kap0 + h * d) - loss(d_kap0 - h * d)) / (2 * h)
+            an = float(torch.dot(g64_d, d))
             fd.append(abs(fdv - an) / abs(an))
+        t_fd = time.perf_counter() - t0
+        fm.finalize()
     m.finalize()
     return {"workload": f"adjoint of L=1/2||x-x_target||^2, 3D Q1 diffusion {n}^3 nodes, log-normal kappa per element "
                         f"({n_elem} elements), forward/adjoint CG+DIAG to 1e-10",
             "assembly_s": t_asm, "loss": 0.5 * float(np.dot(x_ref - target, x_ref - target)), **res,
-            "fd_directions": len(fd), "fd_max_rel_err_fp64": max(fd) if fd else None}
+            "fd_directions": len(fd), "fd_max_rel_err_fp64": max(fd) if fd else None,
+            "fd_median_rel_err_fp64": float(np.median(fd)) if fd else None, "fd_s": t_fd,
+            "fd_solves": ({"count": len(fd_solves), "status_nonzero": sum(1 for q in fd_solves if q[0]),
+                           "iterations_max": max(q[1] for q in fd_solves),
+                           "rel_residual_max": max(q[2] for q in fd_solves)} if fd else None),
+            "fd_method": "central differences, h = 1e-4 along kappa * N(0,1) directions; each side assembled on "
+                         "the device (scaled element matrices + Dirichlet face) and solved to 1e-11 in FP64",
+            "roofline": c5_roofline}
 
 
 def shared_config(n, nz, unknowns):
@@ -744,7 +805,7 @@ def main():
     ap.add_argument("--c3-n", type=int, default=256)
     ap.add_argument("--c3-peclet", type=float, nargs="+", default=[0.5, 5.0, 50.0])
     ap.add_argument("--c5-n", type=int, default=128)
-    ap.add_argument("--c5-fd-dirs", type=int, default=2)
+    ap.add_argument("--c5-fd-dirs", type=int, default=32)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -998,6 +1059,27 @@ def main_ours(args, world, rank, local):
     t_mixed_max = max_over_ranks(t_mixed, world)
     e2e64_max = max_over_ranks(float(np.mean(e2e64)), world)
 
+    workloads = {}
+    if args.c4_sharded:
+        try:
+            workloads["c4_sharded"] = workload_c4_sharded(lib, args, rank, world)
+        except Exception as e:  # report, do not hide
+            workloads["c4_sharded"] = {"failed": repr(e)}
+    if rank == 0 and world == 1:
+        for w in [w for w in args.workloads.split(",") if w and w != "none"]:
+            try:
+                if w == "c3":
+                    workloads["c3"] = workload_c3(lib, args, peak)
+                elif w == "c5":
+                    workloads["c5"] = workload_c5(lib, args)
+                elif w == "c4":
+                    workloads["c4"] = workload_c4(lib, args)
+            except Exception as e:  # report, do not hide
+                workloads[w] = {"failed": repr(e)}
+            log(f"[rank 0] workload {w}: {json.dumps(workloads[w])[:400]}")
+
+    # the CPU baseline last: its OpenMP threads would otherwise share the
+    # host cores with the graph-launching threads of the GPU workloads
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -1024,25 +1106,6 @@ def main_ours(args, world, rank, local):
             mo.finalize()
         except Exception as e:  # report, do not hide
             cpu = {"value": None, "unit": "s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
-
-    workloads = {}
-    if args.c4_sharded:
-        try:
-            workloads["c4_sharded"] = workload_c4_sharded(lib, args, rank, world)
-        except Exception as e:  # report, do not hide
-            workloads["c4_sharded"] = {"failed": repr(e)}
-    if rank == 0 and world == 1:
-        for w in [w for w in args.workloads.split(",") if w and w != "none"]:
-            try:
-                if w == "c3":
-                    workloads["c3"] = workload_c3(lib, args, peak)
-                elif w == "c5":
-                    workloads["c5"] = workload_c5(lib, args)
-                elif w == "c4":
-                    workloads["c4"] = workload_c4(lib, args)
-            except Exception as e:  # report, do not hide
-                workloads[w] = {"failed": repr(e)}
-            log(f"[rank 0] workload {w}: {json.dumps(workloads[w])[:400]}")
 
     if rank == 0:
         spmv32_bytes = layout_bytes["fp32"]

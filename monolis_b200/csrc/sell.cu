@@ -230,7 +230,7 @@ __global__ void diag_setup_kernel(const int* __restrict__ rowptr, const int* __r
 // product, or with a persistent grid when the unroll depth is tuned for the
 // solver kernels, which all run persistent grids.
 template <int B, int U, class V, class T>
-__global__ void __launch_bounds__(256) spmv_kernel(SellView<V> A, const T* __restrict__ x, T* __restrict__ y) {
+__global__ void __launch_bounds__(256, SpmvMinBlocks<B>::value) spmv_kernel(SellView<V> A, const T* __restrict__ x, T* __restrict__ y) {
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
     T acc[B];
     sell_row<B, U, V, T>(A, x, row, acc);
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(256) spmv_kernel(SellView<V> A, const T* __res
 }
 
 template <int B, int U>
-__global__ void __launch_bounds__(256) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
+__global__ void __launch_bounds__(256, SpmvMinBlocks<B>::value) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; 2 * t < A.N; t += gridDim.x * blockDim.x) {
     float y0[B], y1[B];
     sell_row2<B, U>(A, x, t, y0, y1);

@@ -211,7 +211,7 @@ __device__ void fin_grop(SolverState* st, double g1, double rr, double* hist) {
 // with iter % iter_RR == 0, after the update kernel has raised rr_flag.
 // ---------------------------------------------------------------------------
 template <int B, int U, class V, class T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     resid_kernel(SellView<V> A, const T* __restrict__ x, const T* __restrict__ b, T* __restrict__ r,
                  T* __restrict__ z, T* __restrict__ rt, const T* __restrict__ alu, int prec, int mode,
                  double* partials, unsigned int* ticket, SolverState* st, double* hist) {
@@ -294,7 +294,7 @@ __global__ void cg_p_kernel(long long n, T* __restrict__ p, const T* __restrict_
 
 // Q = A P fused with omega = <P,Q>, alpha = rho/omega (CG.f90:85-87).
 template <int B, int U, class V, class T, bool kSet = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     cg_spmv_kernel(SellView<V> A, const T* __restrict__ p, T* __restrict__ q, double* partials,
                    unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // out = A in (no dot)
 template <int B, int U, class V, class T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     pipe_spmv_kernel(SellView<V> A, const T* __restrict__ in, T* __restrict__ out, const SolverState* st) {
   if (st->done) return;
   for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < A.N; row += gridDim.x * blockDim.x) {
@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // V = A U, P = beta P + U, S = beta S + V (one rank: V is not stored)
 template <int B, int U, class V, class T>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     grop_spmv_kernel(SellView<V> A, const T* __restrict__ u, T* __restrict__ p, T* __restrict__ s,
                      const SolverState* st) {
   if (st->done) return;
@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // V = A PT; c2 = <RT,V>; alpha = rho/c2 (BiCGSTAB.f90:113-123)
 template <int B, int U, class V, class T, bool kSet = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     bicg_v_kernel(SellView<V> A, const T* __restrict__ pt, T* __restrict__ vv, const T* __restrict__ rt,
                   double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // T = A ST; (T,S), (T,T); omega = (T,S)/(T,T) or 0 (BiCGSTAB.f90:128-146)
 template <int B, int U, class V, class T, bool kSet = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     bicg_t_kernel(SellView<V> A, const T* __restrict__ stv, T* __restrict__ t, const T* __restrict__ s,
                   double* partials, unsigned int* ticket, SolverState* st, RowSet rs, int acc) {
   if (st->done) return;
@@ -966,7 +966,7 @@ __device__ void fin_mixed_bicg(SolverState* st, double rr, double rrt, double* h
 
 // V = A PT (FP32 paired layout); c2 = <RT,V>; alpha = rho/c2.
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     mbicg_v_kernel(SellView2 A, const float* __restrict__ pt, float* __restrict__ vv, const float* __restrict__ rt,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
@@ -998,7 +998,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // T = A ST (FP32 paired layout); (T,S), (T,T); omega.
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     mbicg_t_kernel(SellView2 A, const float* __restrict__ stv, float* __restrict__ t, const float* __restrict__ s,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
@@ -1080,7 +1080,7 @@ __global__ void mixed_p_kernel(long long n, float* __restrict__ p, const float* 
 
 // FP32 paired-layout SpMV fused with <P,Q> (mixed precision inner loop).
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     cg_spmv2_kernel(SellView2 A, const float* __restrict__ p, float* __restrict__ q, double* partials,
                     unsigned int* ticket, SolverState* st) {
   if (st->done) return;
@@ -1198,7 +1198,7 @@ struct XPlusY {
 // BiCGSTAB mode (Bicg): the second dot is <r,rt> and the initial refresh
 // also sets the shadow residual rt = r (z unused).
 template <int B, int U, bool Bicg = false>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     mixed_refresh_kernel(SellView<double> A, const double* __restrict__ x, const float* __restrict__ y,
                          const double* __restrict__ b, float* __restrict__ r, float* __restrict__ z,
                          const float* __restrict__ alu, int prec, double* partials, unsigned int* ticket,

@@ -354,6 +354,17 @@ __device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int r
   diag_solve<B, T>([&](int j, int k) { return alu[(long long)(j * B + k) * N + row]; }, t);
 }
 
+// Resident blocks of 256 threads per SM that the SpMV kernels are compiled
+// for. With 1x1 blocks a row has few slots and the kernels are bound by
+// memory latency, not bandwidth: at 256^3 (7 entries a row) six blocks per
+// SM (40 registers) stream the FP64 SELL matrix at 5.7 TB/s where four
+// (56-64 registers) reach 4.9 TB/s, with the same per-row order and bits.
+// Larger blocks keep the compiler's choice.
+template <int B>
+struct SpmvMinBlocks {
+  static constexpr int value = B == 1 ? 6 : 1;
+};
+
 // Compile-time block size and unroll depth from their runtime values.
 template <class F>
 inline int dispatch_ndof(int ndof, F&& f) {
