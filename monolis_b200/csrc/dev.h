@@ -173,6 +173,7 @@ void shard_comm_destroy(void* comm);
 int shard_setup(ShardPlan& sp, const ShardTables& t, int ndof, const SellMatrix& A, cudaStream_t s);
 void shard_free(ShardPlan& sp);
 int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s);
+int shard_halo(const ShardPlan& sp, float* v, cudaStream_t s);  // FP32 vectors (refined solve)
 // halo update of v on the side stream, ordered after the work already on s;
 // shard_halo_join makes s wait for it
 int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s);

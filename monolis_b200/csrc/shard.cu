@@ -227,13 +227,23 @@ void shard_free(ShardPlan& sp) {
   sp = ShardPlan();
 }
 
-// Ghost entries of v (FP64, block rows of ndof) from their owners.
-int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) {
+namespace {
+template <class T>
+constexpr ncclDataType_t nccl_type();
+template <>
+constexpr ncclDataType_t nccl_type<double>() { return ncclDouble; }
+template <>
+constexpr ncclDataType_t nccl_type<float>() { return ncclFloat; }
+
+// Ghost entries of v (block rows of ndof) from their owners. The staging
+// buffers hold ndof doubles per listed row, so FP32 vectors fit as well.
+template <class T>
+int halo_update(const ShardPlan& sp, T* v, cudaStream_t s) {
   NcclApi& a = nccl();
   const int nd = sp.ndof;
-  double* sb = static_cast<double*>(sp.d_sendbuf);
-  double* rb = static_cast<double*>(sp.d_recvbuf);
-  if (sp.n_send > 0) pack_kernel<double><<<148 * 2, 256, 0, s>>>(v, sp.d_send_item, sp.n_send, nd, sb);
+  T* sb = static_cast<T*>(sp.d_sendbuf);
+  T* rb = static_cast<T*>(sp.d_recvbuf);
+  if (sp.n_send > 0) pack_kernel<T><<<148 * 2, 256, 0, s>>>(v, sp.d_send_item, sp.n_send, nd, sb);
   // the list this rank sends to itself lands directly in its receive buffer
   for (size_t q = 0; q < sp.send_pe.size(); q++) {
     if (sp.send_pe[q] != sp.rank) continue;
@@ -242,7 +252,7 @@ int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) {
       const size_t cnt = (size_t)(sp.send_ptr[q + 1] - sp.send_ptr[q]) * nd;
       if (cnt)
         MB_CUDA_OK(cudaMemcpyAsync(rb + (size_t)sp.recv_ptr[r] * nd, sb + (size_t)sp.send_ptr[q] * nd,
-                                   cnt * sizeof(double), cudaMemcpyDeviceToDevice, s));
+                                   cnt * sizeof(T), cudaMemcpyDeviceToDevice, s));
     }
   }
   bool remote = false;
@@ -253,22 +263,26 @@ int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) {
     for (size_t q = 0; !rc && q < sp.send_pe.size(); q++) {
       if (sp.send_pe[q] == sp.rank) continue;
       const size_t off = (size_t)sp.send_ptr[q] * nd, cnt = (size_t)(sp.send_ptr[q + 1] - sp.send_ptr[q]) * nd;
-      rc = nccl_check(a.Send(sb + off, cnt, ncclDouble, sp.send_pe[q], static_cast<ncclComm_t>(sp.comm), s),
+      rc = nccl_check(a.Send(sb + off, cnt, nccl_type<T>(), sp.send_pe[q], static_cast<ncclComm_t>(sp.comm), s),
                       "ncclSend");
     }
     for (size_t q = 0; !rc && q < sp.recv_pe.size(); q++) {
       if (sp.recv_pe[q] == sp.rank) continue;
       const size_t off = (size_t)sp.recv_ptr[q] * nd, cnt = (size_t)(sp.recv_ptr[q + 1] - sp.recv_ptr[q]) * nd;
-      rc = nccl_check(a.Recv(rb + off, cnt, ncclDouble, sp.recv_pe[q], static_cast<ncclComm_t>(sp.comm), s),
+      rc = nccl_check(a.Recv(rb + off, cnt, nccl_type<T>(), sp.recv_pe[q], static_cast<ncclComm_t>(sp.comm), s),
                       "ncclRecv");
     }
     const int rc2 = nccl_check(a.GroupEnd(), "ncclGroupEnd");
     if (rc || rc2) return rc ? rc : rc2;
   }
-  if (sp.n_recv > 0) unpack_kernel<double><<<148 * 2, 256, 0, s>>>(v, sp.d_recv_item, sp.n_recv, nd, rb);
+  if (sp.n_recv > 0) unpack_kernel<T><<<148 * 2, 256, 0, s>>>(v, sp.d_recv_item, sp.n_recv, nd, rb);
   MB_CUDA_OK(cudaGetLastError());
   return kOk;
 }
+}  // namespace
+
+int shard_halo(const ShardPlan& sp, double* v, cudaStream_t s) { return halo_update<double>(sp, v, s); }
+int shard_halo(const ShardPlan& sp, float* v, cudaStream_t s) { return halo_update<float>(sp, v, s); }
 
 int shard_halo_fork(const ShardPlan& sp, double* v, cudaStream_t s) {
   MB_CUDA_OK(cudaEventRecord(sp.ev_fork, s));

@@ -1031,7 +1031,8 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
 // P = Z + beta*P in FP32 (P = Z on iteration 1), and after a refresh the
 // fold of the FP32 correction into the FP64 solution: X += Y, Y = 0.
 __global__ void mixed_p_kernel(long long n, float* __restrict__ p, const float* __restrict__ z,
-                               double* __restrict__ x, float* __restrict__ y, const SolverState* st) {
+                               double* __restrict__ x, float* __restrict__ y, const SolverState* st,
+                               long long n_fold = 0) {
   if (st->done) return;
   const bool first = st->iter == 1;
   const bool fold = st->fold != 0;
@@ -1076,6 +1077,12 @@ __global__ void mixed_p_kernel(long long n, float* __restrict__ p, const float* 
       y[i] = 0.0f;
     }
   }
+  // several ranks: the ghost rows of x and y follow their owners' (same fold)
+  if (fold)
+    for (long long i = n + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_fold; i += stride) {
+      x[i] += (double)y[i];
+      y[i] = 0.0f;
+    }
 }
 
 // FP32 paired-layout SpMV fused with <P,Q> (mixed precision inner loop).
@@ -1105,6 +1112,10 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     }
   }
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // alpha after the all-reduce (shard_mixed_alpha_kernel)
+      st->red[0] = tot[0];
+      return;
+    }
     st->omega = tot[0];
     st->alpha = st->rho / tot[0];
     st->fold = 0;  // the p kernel of this iteration has folded y
@@ -1118,7 +1129,7 @@ template <int B>
 __global__ void __launch_bounds__(kThreads)
     mixed_update_kernel(int N, float* __restrict__ y, const float* __restrict__ p, float* __restrict__ r,
                         const float* __restrict__ q, float* __restrict__ z, const float* __restrict__ alu, int prec,
-                        double* partials, unsigned int* ticket, SolverState* st, double* hist) {
+                        double* partials, unsigned int* ticket, SolverState* st, double* hist, int n_ext_rows = 0) {
   using RG = RowGroup<float, B>;
   constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
@@ -1180,7 +1191,68 @@ __global__ void __launch_bounds__(kThreads)
       v.add(1, t[c], w[c]);
     }
   }
-  grid_reduce<2>(v, partials, ticket, [&](double* tot) { fin_mixed_inner(st, tot[0], tot[1], hist); });
+  // several ranks: y of the ghost rows follows its owner's (p's ghost entries
+  // hold the owner's values after this iteration's halo update), so x + y is
+  // valid on the ghost rows whenever the FP64 refresh multiplies it
+  for (long long i = (long long)N * B + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+       i < (long long)n_ext_rows * B; i += stride)
+    y[i] = fmaf(alpha, p[i], y[i]);
+  grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // fin_mixed_inner after the all-reduce (shard_mixed_inner_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
+    fin_mixed_inner(st, tot[0], tot[1], hist);
+  });
+}
+
+// End of a refresh (or of the initial residual when iter == 0): rr = <r64,r64>,
+// rz = <r,z> (CG) or <r,rt> (BiCGSTAB).
+template <bool Bicg>
+__device__ void fin_mixed_refresh(SolverState* st, double rr, double rz, double* hist) {
+  if (st->iter == 0) {
+    st->B2 = rr;
+    if (rr == 0.0) { st->done = 1; st->status = kZeroRhs; return; }
+    st->rmax = sqrt(rr);
+    st->rho = rz;
+    st->iter = 1;
+    return;
+  }
+  const double resid = sqrt(rr / st->B2);
+  record(st, hist, resid);
+  st->refresh = 0;
+  st->fold = 1;
+  st->n_refine += 1;
+  st->last_refresh = st->iter;
+  if (resid < st->tol) { st->done = 1; st->status = kOk; return; }
+  if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
+  if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
+  st->rmax = sqrt(rr);
+  st->rho = rz;
+  if (Bicg) {
+    if (rz == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+    st->beta = (st->rho / st->rho1) * (st->alpha / st->omega);
+  } else {
+    st->beta = st->rho / st->rho1;
+  }
+  st->iter += 1;
+}
+
+// Multi-rank FP32-refined CG: the scalar steps with the all-reduced sums in red[].
+__global__ void shard_mixed_alpha_kernel(SolverState* st) {
+  if (st->done) return;
+  st->omega = st->red[0];
+  st->alpha = st->rho / st->red[0];
+  st->fold = 0;
+}
+__global__ void shard_mixed_inner_kernel(SolverState* st, double* hist) {
+  if (st->done) return;
+  fin_mixed_inner(st, st->red[0], st->red[1], hist);
+}
+__global__ void shard_mixed_refresh_kernel(SolverState* st, double* hist) {
+  if (st->done || !(st->iter == 0 || st->refresh)) return;
+  fin_mixed_refresh<false>(st, st->red[0], st->red[1], hist);
 }
 
 // Refresh: r64 = b - A64 (x + y) with the FP64 matrix, r = fp32(r64),
@@ -1239,33 +1311,12 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
-    const double rr = tot[0], rz = tot[1];
-    if (st->iter == 0) {
-      st->B2 = rr;
-      if (rr == 0.0) { st->done = 1; st->status = kZeroRhs; return; }
-      st->rmax = sqrt(rr);
-      st->rho = rz;
-      st->iter = 1;
+    if (st->sharded) {  // the finish after the all-reduce (shard_mixed_refresh_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
       return;
     }
-    const double resid = sqrt(rr / st->B2);
-    record(st, hist, resid);
-    st->refresh = 0;
-    st->fold = 1;
-    st->n_refine += 1;
-    st->last_refresh = st->iter;
-    if (resid < st->tol) { st->done = 1; st->status = kOk; return; }
-    if (!isfinite(resid)) { st->done = 1; st->status = kNonFinite; return; }
-    if (st->iter >= st->max_iter) { st->done = 1; st->status = kMaxIter; return; }
-    st->rmax = sqrt(rr);
-    st->rho = rz;
-    if (Bicg) {
-      if (rz == 0.0) { st->done = 1; st->status = kBreakdown; return; }
-      st->beta = (st->rho / st->rho1) * (st->alpha / st->omega);
-    } else {
-      st->beta = st->rho / st->rho1;
-    }
-    st->iter += 1;
+    fin_mixed_refresh<Bicg>(st, tot[0], tot[1], hist);
   });
 }
 
@@ -1329,8 +1380,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     fprintf(stderr, "** monolis_b200: GropCG and PipeCG run in FP64\n");
     return kBadInput;
   }
-  if (p.shard && (p.precision != 0 || p.np_rows < N)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB)\n");
+  if (p.shard && ((p.precision != 0 && p.method != 1) || p.np_rows < N)) {
+    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG\n");
     return kBadInput;
   }
   // vectors gathered by the SpMV hold the ghost rows too
@@ -1740,6 +1791,59 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (ev) cudaEventRecord(ev[6], ss);
       };
       plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n, x, y, st); };
+    } else if (p.shard) {
+      // multi-rank FP32-refined CG: halo update of p (FP32) before the product,
+      // every dot product all-reduced, the refresh's all-reduce in every
+      // iteration (the refresh is decided on the device, from all-reduced
+      // sums, identically on every rank). The ghost rows of y and x are
+      // updated with the owners' arithmetic (y += alpha p after p's halo
+      // update, the folds), so the FP64 refresh multiplies x + y on the
+      // ghost rows without a halo update of its own.
+      const ShardPlan* sp = p.shard;
+      SellView2 A32 = view2_of(m);
+      const float* alu32 = m.d_alu32;
+      float *r = vec.get<float>(n), *z = vec.get<float>(n), *q = vec.get<float>(n), *pp = vec.get<float>(n_ext),
+            *y = vec.get<float>(n_ext);
+      if (!r || !z || !q || !pp || !y) return kCudaError;
+      double* x = d_x;
+      const double* b = d_b;
+      const int NP = p.np_rows;
+      auto k_spmv = cg_spmv2_kernel<B, U>;
+      auto k_upd = mixed_update_kernel<B>;
+      auto k_ref = mixed_refresh_kernel<B, U>;
+      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd), g_ref = pgrid(k_ref);
+      if (cudaMemsetAsync(y, 0, sizeof(float) * n_ext, s) != cudaSuccess) return kCudaError;
+      if (cudaMemsetAsync(pp, 0, sizeof(float) * n_ext, s) != cudaSuccess) return kCudaError;
+      int rc2 = shard_halo(*sp, x, s);
+      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
+      if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+      shard_mixed_refresh_kernel<<<1, 1, 0, s>>>(st, hist);
+      if (rc2) return rc2;
+      const int hk = (sp->n_send > 0) + (sp->n_recv > 0);
+      plan.kernels = 4;
+      plan.always_all = true;
+      plan.launches = 7 + hk;
+      plan.launches_special = 7 + hk;
+      plan.kind = {1, 0, 2, 0};
+      plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
+        if (ev) cudaEventRecord(ev[0], ss);
+        mixed_p_kernel<<<gvec, kThreads, 0, ss>>>(n, pp, z, x, y, st, n_ext);
+        if (ev) cudaEventRecord(ev[1], ss);
+        shard_halo(*sp, pp, ss);
+        k_spmv<<<g_spmv, kThreads, 0, ss>>>(A32, pp, q, partials, ticket, st);
+        shard_allreduce(*sp, st->red, 1, ss);
+        shard_mixed_alpha_kernel<<<1, 1, 0, ss>>>(st);
+        if (ev) cudaEventRecord(ev[2], ss);
+        k_upd<<<g_upd, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist, NP);
+        shard_allreduce(*sp, st->red, 2, ss);
+        shard_mixed_inner_kernel<<<1, 1, 0, ss>>>(st, hist);
+        if (ev) cudaEventRecord(ev[3], ss);
+        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
+        shard_allreduce(*sp, st->red, 2, ss);
+        shard_mixed_refresh_kernel<<<1, 1, 0, ss>>>(st, hist);
+        if (ev) cudaEventRecord(ev[4], ss);
+      };
+      plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n_ext, x, y, st); };
     } else {
       SellView2 A32 = view2_of(m);
       const float* alu32 = m.d_alu32;
@@ -1764,7 +1868,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (ev) cudaEventRecord(ev[1], ss);
         k_spmv<<<g_spmv, kThreads, 0, ss>>>(A32, pp, q, partials, ticket, st);
         if (ev) cudaEventRecord(ev[2], ss);
-        k_upd<<<g_upd, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist);
+        k_upd<<<g_upd, kThreads, 0, ss>>>(N, y, pp, r, q, z, alu32, prec, partials, ticket, st, hist, 0);
         if (ev) cudaEventRecord(ev[3], ss);
         k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
         if (ev) cudaEventRecord(ev[4], ss);
@@ -1898,6 +2002,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   if (plan.finalize) {
     plan.finalize(s);
     launched_kernels += 1;
+  }
+  // several ranks: the ghost entries of the solution from their owners, as
+  // the reference's solvers end (src/iterative/CG.f90:105,
+  // BiCGSTAB.f90:174, GropCG.f90:121); every rank reaches this point
+  if (p.shard) {
+    rc = shard_halo(*p.shard, d_x, s);
+    if (rc) return rc;
   }
   SolverState fin{};
   err = read_state(fin);

@@ -63,8 +63,8 @@ def test_sharded_path_rejects_unsupported(gpu):
     ms.set_error_abort(False)
     ms.set_halo(p, 0, 1)
     ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
-    _, _, _, st = solve(ms, b, api.ITER_CG, api.PREC_DIAG, precision=1)
-    assert st == 5  # the multi-rank solve is FP64 (CG or BiCGSTAB)
+    _, _, _, st = solve(ms, b, api.ITER_BICGSTAB, api.PREC_DIAG, precision=1)
+    assert st == 5  # on several ranks the FP32-refined form is CG only
     ms.finalize()
 
 
@@ -120,6 +120,9 @@ def test_sharded_boundary_rows_through_self_halo(gpu, problem, kw, method):
     assert sts == 0
     assert abs(its - it_ref) <= 2, (its, it_ref)
     assert np.linalg.norm(xs[:N * nd] - x_ref) / np.linalg.norm(x_ref) < 1e-9
+    # the solve ends with the ghost entries of x updated from their owners
+    # (src/iterative/CG.f90:105 and the other solvers' last step)
+    assert bits_equal(xs[N * nd:].reshape(-1, nd), xs[:N * nd].reshape(-1, nd)[mirrored])
     ms.finalize()
 
 
@@ -162,4 +165,88 @@ def test_device_solve_com_one_rank(gpu, problem, kw, method):
     assert ms.device_solve_com(d_b.data_ptr(), d_x2.data_ptr()) == 0
     assert ms.get_converge_iter() == it_ref
     assert bits_equal(d_x2.cpu().numpy(), x_ref)
+    ms.finalize()
+
+
+@pytest.mark.parametrize("problem,kw,tol", [
+    ("elasticity", dict(n=12), 1e-8),
+    ("laplacian", dict(n=20), 1e-10),
+    ("diffusion_kappa", dict(n=10), 1e-9),
+])
+def test_sharded_mixed_cg_one_rank_bit_identical(gpu, problem, kw, tol):
+    """The multi-rank FP32-refined CG (FP32 halo update of p, all-reduced dot
+    products, the refresh's all-reduce in every iteration, y and x kept on
+    the ghost rows) through a one-rank NCCL communicator: the iteration
+    count, residual, refresh count and solution bits of the plain refined
+    solve."""
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    xp, itp, resp, stp = solve(mp, b, api.ITER_CG, api.PREC_DIAG, tol=tol, precision=1)
+    assert stp == 0 and resp < tol
+    nref = mp.Iarray[api.B200_PRM_I_N_REFINE]
+    p = partition.partition_rank(mp.csr_index(), mp.csr_item() - 1, mp.values(), nd, 1, 0)
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(p["N"], p["NP"], nd, len(p["item"]), p["val"], p["index"], p["item"])
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_halo(p, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    xs, its, ress, sts = solve(ms, b, api.ITER_CG, api.PREC_DIAG, tol=tol, precision=1)
+    assert sts == 0
+    assert its == itp and ress == resp and ms.Iarray[api.B200_PRM_I_N_REFINE] == nref
+    assert bits_equal(xs, xp)
+    ms.finalize()
+
+
+@pytest.mark.parametrize("problem,kw", [("laplacian", dict(n=14)), ("elasticity", dict(n=7))])
+def test_sharded_mixed_cg_through_self_halo(gpu, problem, kw):
+    """FP32-refined CG on a one-rank system whose rows read every 7th node
+    through a ghost copy (filled by a self-exchange): the FP64 refreshes
+    multiply x + y on the ghost rows, which the solver keeps with the owners'
+    arithmetic; the solution reaches the tolerance on the FP64 residual of
+    the original system and matches the plain refined solve to it."""
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    N = mp.N
+    tol = 1e-10
+    x_ref, it_ref, _, st = solve(mp, b, api.ITER_CG, api.PREC_DIAG, tol=tol, precision=1)
+    assert st == 0
+    index = mp.csr_index().astype(np.int64)
+    item = (mp.csr_item() - 1).astype(np.int64)
+    val = mp.values().reshape(-1, nd * nd)
+    mirrored = np.arange(3, N, 7)
+    ghost = np.full(N, -1, dtype=np.int64)
+    ghost[mirrored] = N + np.arange(len(mirrored))
+    NP = N + len(mirrored)
+    new_index, new_item, new_val = [0], [], []
+    for i in range(N):
+        cols = item[index[i]:index[i + 1]]
+        cols2 = np.where((ghost[cols] >= 0) & (cols != i), ghost[cols], cols)
+        order = np.argsort(cols2, kind="stable")
+        new_item.extend(cols2[order].tolist())
+        new_val.append(val[index[i]:index[i + 1]][order])
+        new_index.append(len(new_item))
+    new_index += [new_index[-1]] * (NP - N)
+    new_val = np.concatenate(new_val).reshape(-1)
+    halo = {"N": N, "recv_pe": [0], "recv_index": [0, len(mirrored)], "recv_item": np.arange(N, NP),
+            "send_pe": [0], "send_index": [0, len(mirrored)], "send_item": mirrored}
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(N, NP, nd, len(new_item), new_val, np.array(new_index, dtype=np.int32),
+                       np.array(new_item, dtype=np.int32))
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_halo(halo, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    bl = np.zeros(NP * nd)
+    bl[:N * nd] = b
+    xs, its, ress, sts = solve(ms, bl, api.ITER_CG, api.PREC_DIAG, tol=tol, precision=1)
+    assert sts == 0 and ress < tol
+    assert ms.Iarray[api.B200_PRM_I_N_REFINE] >= 1
+    x = xs[:N * nd]
+    # the FP64 residual of the original (unmirrored) system
+    assert np.linalg.norm(b - mp.matvec(x)) / np.linalg.norm(b) < 1.01 * tol
+    assert abs(its - it_ref) <= max(3, it_ref // 10), (its, it_ref)
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-7
+    # the solve ends with the ghost entries of x updated from their owners
+    assert bits_equal(xs[N * nd:].reshape(-1, nd), xs[:N * nd].reshape(-1, nd)[mirrored])
     ms.finalize()
