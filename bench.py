@@ -832,10 +832,14 @@ def main_sharded(args, world, rank, local):
     in the same order, whatever happens locally."""
     import datetime
 
-    # NCCL's own log of every communicator (ranks, devices, transports) on
-    # stderr, before the process group or the library creates one
-    os.environ.setdefault("NCCL_DEBUG", "INFO")
-    os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
+    # NCCL's own log of every communicator (ranks, devices, transports),
+    # before the process group or the library creates one. NCCL writes it to
+    # the process's stdout; that descriptor is pointed at stderr, and the one
+    # JSON line goes to the original stdout.
+    os.environ["NCCL_DEBUG"] = "INFO"
+    sys.stdout.flush()
+    json_out = os.fdopen(os.dup(1), "w")
+    os.dup2(2, 1)
     import torch
     import torch.distributed as dist
 
@@ -911,6 +915,21 @@ def main_sharded(args, world, rank, local):
     it = int(np.median(iters))
     res = m.get_converge_residual()
     launches = int(m.Iarray[api.B200_PRM_I_LAUNCHES]) * args.steps
+    # the FP32-refined CG on the same partition (FP32 halo of p, all-reduced dots)
+    m.set_precision(1)
+    m.device_prepare()
+    barrier()
+    t32, it32, failed32 = [], [], None
+    for k in range(1 + args.steps):
+        t, rc = one()
+        failed32 = failed32 or (rc or None)
+        if k >= 1:
+            t32.append(t)
+            it32.append(m.get_converge_iter())
+    barrier()
+    t32_max = max_over_ranks(float(np.mean(t32)) if failed32 is None else float("inf"), world)
+    nref32 = int(m.Iarray[api.B200_PRM_I_N_REFINE])
+    m.set_precision(0)
     # e2e: monolis_solve_R with this rank's host b and x (pinned), device matrix kept
     hb = torch.from_numpy(b_loc).pin_memory()
     hx = torch.zeros(len(b_loc), dtype=torch.float64).pin_memory()
@@ -933,6 +952,10 @@ def main_sharded(args, world, rank, local):
             "parallelism": f"row partition over {world} ranks (z-slabs; NCCL halo updates + all-reduced dots)",
             "statistic": f"mean of {len(times)} solves, max over ranks", "iterations": it, "rel_residual": res,
             "failed_status": failed,
+            "mixed": {"value": t32_max, "unit": "s", "dtype": "f32 inner / f64 refinement",
+                      "iterations": int(np.median(it32)), "fp64_refreshes": nref32, "failed_status": failed32,
+                      "statistic": f"mean of {len(t32)} solves after one untimed, max over ranks"},
+            "speedup_mixed_vs_fp64": t_max / t32_max,
             "rank0": {"rows": int(p["N"]), "ghost_rows": int(p["NP"] - p["N"]),
                       "neighbours": [int(v) for v in p["recv_pe"]], "step_s": times},
             "e2e": {"value": e2e_max, "unit": "s",
@@ -945,7 +968,7 @@ def main_sharded(args, world, rank, local):
             "roofline": None, "roofline_note": "see the one-GPU line (the same kernels on 1/N of the rows)",
             "cpu_baseline": None, "peak_gbs": peak, "peak_kind": peak_kind,
         }
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line), file=json_out, flush=True)
     m.finalize()
     if world > 1:
         dist.destroy_process_group()
