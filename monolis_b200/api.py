@@ -366,6 +366,10 @@ class Monolis:
         if rc:
             raise ValueError(f"bad precision {p}")
 
+    def matrix_changed(self):
+        """monolis_b200_matrix_changed: the host arrays were written directly."""
+        self.lib.monolis_b200_matrix_changed(self.p)
+
     def set_matrix_cache(self, b):
         self.lib.monolis_b200_set_matrix_cache(self.p, bool(b))
 
