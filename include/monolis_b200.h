@@ -50,6 +50,9 @@ static const int MONOLIS_B200_PRM_I_WAIT_LIMIT     = 44; /* many right-hand side
 static const int MONOLIS_B200_PRM_I_WAIT_DELAY_US  = 45; /* testing that bound: block 0 of the many-right-hand-side
                                                             kernel reaches its first barrier this many microseconds
                                                             late (0: off; at most 1,000,000) */
+static const int MONOLIS_B200_PRM_I_UNIFORM_SLICES_FP64 = 46; /* out: 32-row slices whose block columns are the
+                                                            per-slot base plus the lane (no column stream read) */
+static const int MONOLIS_B200_PRM_I_UNIFORM_SLICES_FP32 = 47; /* out: same for the 64-row slices of the FP32 layout */
 
 static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
                                                             below delta * its largest value since the last one

@@ -57,6 +57,8 @@ B200_PRM_I_WIDE_SLICES_FP64 = 42
 B200_PRM_I_WIDE_SLICES_FP32 = 43
 B200_PRM_I_WAIT_LIMIT = 44
 B200_PRM_I_WAIT_DELAY_US = 45
+B200_PRM_I_UNIFORM_SLICES_FP64 = 46
+B200_PRM_I_UNIFORM_SLICES_FP32 = 47
 B200_PRM_R_REFRESH_DELTA = 30
 B200_PRM_R_TIME_H2D = 31
 B200_PRM_R_TIME_D2H = 32

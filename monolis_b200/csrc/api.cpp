@@ -401,6 +401,8 @@ int prepare(MONOLIS* m, DevState* s, bool need_diag, bool need_fp32, double* t_h
   m->prm.Iarray[MONOLIS_B200_PRM_I_UNROLL_FP32] = s->A.have_val32 ? s->A.u32 : 0;
   m->prm.Iarray[MONOLIS_B200_PRM_I_WIDE_SLICES_FP64] = (int)s->A.wide64;
   m->prm.Iarray[MONOLIS_B200_PRM_I_WIDE_SLICES_FP32] = s->A.have_val32 ? (int)s->A.wide32 : 0;
+  m->prm.Iarray[MONOLIS_B200_PRM_I_UNIFORM_SLICES_FP64] = (int)s->A.uniform64;
+  m->prm.Iarray[MONOLIS_B200_PRM_I_UNIFORM_SLICES_FP32] = s->A.have_val32 ? (int)s->A.uniform32 : 0;
   m->prm.Rarray[MONOLIS_B200_PRM_R_SPMV_BYTES_FP64] = s->A.bytes64;
   m->prm.Rarray[MONOLIS_B200_PRM_R_SPMV_BYTES_FP32] = s->A.have_val32 ? s->A.bytes32 : 0.0;
   return mb::kOk;

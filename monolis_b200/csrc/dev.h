@@ -18,7 +18,10 @@
 // structured mesh) and small for any locally numbered mesh. A slice whose
 // differences do not all fit in 16 bits keeps reading col[]; slc[s] is
 // slptr[s] with bit 0 set for those slices. The compressed stream is 2 bytes
-// per block plus 4 bytes per slot per warp instead of 4 bytes per block.
+// per block plus 4 bytes per slot per warp instead of 4 bytes per block. A
+// slice whose differences are all zero (every lane's block k at the same
+// offset from its row, the interior of a structured mesh) has bit 1 set and
+// reads only the bases: 4 bytes per slot per warp.
 #pragma once
 
 #include <cstddef>
@@ -55,6 +58,7 @@ struct SolverState {
   int fold;      // mixed: y still to be folded into x
   int n_refine;  // mixed: refreshes done
   int sharded;   // multi-rank: reductions leave their local sums in red[] for the all-reduce
+  int loops;     // device-side loop: bodies of iterations run (while-node graph)
   double red[4];
 };
 
@@ -83,6 +87,7 @@ struct SellMatrix {
   short* d_col16p = nullptr;
   int* d_cbase2 = nullptr;
   long long wide64 = 0, wide32 = 0;  // slices that keep 32-bit column ids
+  long long uniform64 = 0, uniform32 = 0;  // slices whose columns are the slot bases + lane (bit 1 of slc)
   double bytes64 = 0, bytes32 = 0;   // HBM bytes of one SpMV in each layout
   // unroll depth (slots in flight per thread) picked by the autotuner
   int u64 = 2, u32 = 2;
@@ -104,10 +109,12 @@ struct Scratch {
   double* partials = nullptr;     // (65536 + 256) * 4 doubles: block and group partial sums
   unsigned int* ticket = nullptr;
   SolverState* st = nullptr;
-  SolverState* h_st = nullptr;    // pinned host mirror
+  SolverState* h_st = nullptr;    // pinned host mirror, one slot per launch in flight (8)
   double* hist = nullptr;         // residual history (max_iter + 1)
   size_t hist_cap = 0;
   size_t partials_cap = 0;
+  void* work = nullptr;           // work vectors of the solves (grows to the largest solve's need)
+  size_t work_cap = 0;
 };
 
 // ---- matrix build on the device ----

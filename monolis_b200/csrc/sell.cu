@@ -111,9 +111,14 @@ __global__ void sell_fill_kernel(const int* __restrict__ rowptr, const int* __re
 // column clamp(c0 + P*l + h, 0, N-1), a valid column within 64 of c0 + P*l + h,
 // because the paired layout gathers at padded slots (their values are zero).
 // If any real slot of the slice does not fit, the slice is marked wide (bit 0
-// of slc) and keeps reading col[].
+// of slc) and keeps reading col[]. If every slot of the slice, padded ones
+// included, has difference 0 -- every lane's block k sits at the same offset
+// from its row, as in the interior of a structured mesh -- the slice is
+// marked uniform (bit 1 of slc): its columns are the bases plus the lane
+// position, and the difference stream is not read at all.
 // stats: [0] wide slices, [1] real blocks in wide slices, [2] slot positions
-// of compressed slices.
+// of compressed slices (uniform ones included), [3] real blocks in uniform
+// slices, [4] uniform slices.
 template <int P>
 __global__ void col_compact_kernel(const int* __restrict__ rowptr, const long long* __restrict__ slptr, int N,
                                    int nslices, const int* __restrict__ col, short* __restrict__ col16,
@@ -131,7 +136,7 @@ __global__ void col_compact_kernel(const int* __restrict__ rowptr, const long lo
     const long long row = warp * H + P * lane + h;
     len[h] = row < N ? rowptr[row + 1] - rowptr[row] : 0;
   }
-  bool fit = true;
+  bool fit = true, uni = true;
   unsigned long long nreal = 0;
   for (int k = 0; k < w; k++) {
     const long long slot = base + (long long)k * H;
@@ -162,20 +167,26 @@ __global__ void col_compact_kernel(const int* __restrict__ rowptr, const long lo
         d = tgt - c0 - pos;
       }
       fit = fit && d >= -32768 && d <= 32767;
+      uni = uni && d == 0;
       col16[slot + pos] = (short)d;
     }
     if (lane == 0) cbase[base / H + k] = (int)c0;
   }
   fit = __all_sync(0xffffffffu, fit);
+  uni = __all_sync(0xffffffffu, uni);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) nreal += __shfl_xor_sync(0xffffffffu, nreal, o);
   if (lane == 0) {
-    slc[warp] = base | (fit ? 0 : 1);
+    slc[warp] = base | (fit ? 0 : 1) | (uni ? 2 : 0);
     if (!fit) {
       atomicAdd(&stats[0], 1ULL);
       atomicAdd(&stats[1], nreal);
     } else {
       atomicAdd(&stats[2], (unsigned long long)w);
+      if (uni) {
+        atomicAdd(&stats[3], nreal);
+        atomicAdd(&stats[4], 1ULL);
+      }
     }
   }
 }
@@ -288,29 +299,31 @@ __global__ void diag_apply_kernel(const double* __restrict__ alu, int N, const d
 
 // Compressed column ids for one layout (P rows per lane); returns the column
 // bytes one SpMV streams: 2 per block and 4 per slot position in compressed
-// slices, 4 per block in wide slices.
+// slices, 4 per slot position only in uniform slices, 4 per block in wide
+// slices.
 template <int P>
 int compact_columns(const SellMatrix& m, const long long* d_slptr, int nslices, long long padded,
                     const int* d_col, short** col16, size_t& cap16, int** cbase, size_t& capb, long long** slc,
-                    size_t& capslc, long long& wide, double& col_bytes, cudaStream_t s) {
+                    size_t& capslc, long long& wide, long long& uniform, double& col_bytes, cudaStream_t s) {
   MB_CUDA_OK(grow(col16, cap16, (size_t)padded + 2));
   MB_CUDA_OK(grow(cbase, capb, (size_t)(padded / (32 * P)) + 1));
   MB_CUDA_OK(grow(slc, capslc, (size_t)nslices + 1));
   unsigned long long* d_stats = nullptr;
-  MB_CUDA_OK(cudaMallocAsync((void**)&d_stats, 3 * sizeof(unsigned long long), s));
-  MB_CUDA_OK(cudaMemsetAsync(d_stats, 0, 3 * sizeof(unsigned long long), s));
+  MB_CUDA_OK(cudaMallocAsync((void**)&d_stats, 5 * sizeof(unsigned long long), s));
+  MB_CUDA_OK(cudaMemsetAsync(d_stats, 0, 5 * sizeof(unsigned long long), s));
   if (nslices > 0) {
     const long long threads = (long long)nslices * 32;
     col_compact_kernel<P><<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(m.d_rowptr, d_slptr, m.N, nslices, d_col,
                                                                           *col16, *cbase, *slc, d_stats);
   }
-  unsigned long long st[3] = {0, 0, 0};
+  unsigned long long st[5] = {0, 0, 0, 0, 0};
   MB_CUDA_OK(cudaGetLastError());
   MB_CUDA_OK(cudaMemcpyAsync(st, d_stats, sizeof(st), cudaMemcpyDeviceToHost, s));
   MB_CUDA_OK(cudaStreamSynchronize(s));
   cudaFreeAsync(d_stats, s);
   wide = (long long)st[0];
-  col_bytes = 2.0 * (double)(m.nz - (long long)st[1]) + 4.0 * (double)st[1] + 4.0 * (double)st[2];
+  uniform = (long long)st[4];
+  col_bytes = 2.0 * (double)(m.nz - (long long)st[1] - (long long)st[3]) + 4.0 * (double)st[1] + 4.0 * (double)st[2];
   return kOk;
 }
 
@@ -379,7 +392,7 @@ int sell_layout(SellMatrix& m, cudaStream_t s) {
   MB_CUDA_OK(cudaGetLastError());
   double col_bytes = 0;
   rc = compact_columns<1>(m, m.d_slptr, nslices, m.padded, m.d_col, &m.d_col16, m.cap_col16, &m.d_cbase, m.cap_cbase,
-                          &m.d_slc, m.cap_slc, m.wide64, col_bytes, s);
+                          &m.d_slc, m.cap_slc, m.wide64, m.uniform64, col_bytes, s);
   if (rc) return rc;
   // values, column ids, row offsets, slice offsets, x once and y
   m.bytes64 = (double)m.nz * B2 * 8 + col_bytes + 4.0 * (N + 1) + 8.0 * nslices + 2.0 * N * ndof * 8;
@@ -415,7 +428,7 @@ int sell_make_fp32(SellMatrix& m, cudaStream_t s) {
   MB_CUDA_OK(cudaGetLastError());
   double col_bytes = 0;
   rc = compact_columns<2>(m, m.d_slptr2, ns, m.padded2, m.d_col2, &m.d_col16p, m.cap_col16p, &m.d_cbase2,
-                          m.cap_cbase2, &m.d_slc2, m.cap_slc2, m.wide32, col_bytes, s);
+                          m.cap_cbase2, &m.d_slc2, m.cap_slc2, m.wide32, m.uniform32, col_bytes, s);
   if (rc) return rc;
   m.bytes32 = (double)m.nz * B2 * 4 + col_bytes + 4.0 * (N + 1) + 8.0 * ns + 2.0 * N * m.ndof * 4;
   m.have_val32 = true;
@@ -585,7 +598,7 @@ int scratch_ensure(Scratch& sc, size_t hist_len) {
     MB_CUDA_OK(cudaMemset(sc.ticket, 0, kTicketWords * sizeof(unsigned int)));
   }
   if (!sc.st) MB_CUDA_OK(cudaMalloc((void**)&sc.st, sizeof(SolverState)));
-  if (!sc.h_st) MB_CUDA_OK(cudaMallocHost((void**)&sc.h_st, 4 * sizeof(SolverState)));
+  if (!sc.h_st) MB_CUDA_OK(cudaMallocHost((void**)&sc.h_st, 8 * sizeof(SolverState)));  // launches in flight
   if (sc.hist_cap < hist_len) {
     if (sc.hist) cudaFree(sc.hist);
     MB_CUDA_OK(cudaMalloc((void**)&sc.hist, hist_len * sizeof(double)));
@@ -595,6 +608,7 @@ int scratch_ensure(Scratch& sc, size_t hist_len) {
 }
 
 void scratch_free(Scratch& sc) {
+  cudaFree(sc.work);
   cudaFree(sc.partials);
   cudaFree(sc.ticket);
   cudaFree(sc.st);

@@ -10,12 +10,14 @@
 // a block per 256 rows spends more time entering, reducing and leaving than
 // on its rows.
 //
-// The host captures `batch` iterations into a CUDA graph and launches it
-// repeatedly, reading the state word once per launch with three launches in
-// flight; kernels return immediately once `done` is set. The true residual
-// every iter_RR iterations of FP64 CG/BiCGSTAB falls on the last iteration of
-// a batch (the batch divides iter_RR) and uses a second graph that contains
-// the residual kernel, so no other iteration pays for it. The FP64 refresh of
+// A batch of iterations is captured as the body of a CUDA graph while node
+// whose last kernel lets the body run again until the state word says done,
+// so the whole solve is one graph launch with no host thread in the loop;
+// kernels return immediately once `done` is set. The true residual every
+// iter_RR iterations of FP64 CG/BiCGSTAB falls on the last iteration of a
+// batch (the batch divides iter_RR), whose residual kernel returns at entry
+// unless a replacement is due. Several ranks keep a host-driven loop of batch
+// graphs (every rank must enqueue the same collectives). The FP64 refresh of
 // the mixed solver is decided on the device from the residual history; its
 // kernel sits in every iteration on a small grid and returns at once when
 // there is nothing to do.
@@ -415,6 +417,14 @@ __global__ void __launch_bounds__(kThreads)
     }
     fin_cg(st, tot[0], tot[1], hist);
   });
+}
+
+// Device-side loop control: the last kernel of the body of a while node
+// (one graph for the whole solve) lets the body run again until the solve has
+// a verdict; the iteration cap bounds it even without one.
+__global__ void loop_continue_kernel(cudaGraphConditionalHandle h, SolverState* st, int cap) {
+  st->loops += 1;
+  cudaGraphSetConditional(h, (st->done || st->iter > cap) ? 0u : 1u);
 }
 
 // Multi-rank CG: the scalar updates, with the sums all-reduced over the ranks
@@ -1334,17 +1344,35 @@ __global__ void mixed_fold_kernel(long long n, double* __restrict__ x, float* __
 // ---------------------------------------------------------------------------
 
 
+// Work vectors of one solve, carved in order from the scratch's work arena
+// (kept between solves, so a repeated solve maps no new memory). Vectors
+// past the arena's end are allocated from the stream's pool and freed after
+// the solve; the arena then grows to the whole solve's need for the next one.
 struct Vecs {
-  std::vector<void*> ptrs;
+  Scratch& sc;
   cudaStream_t s;
+  size_t used = 0;
+  std::vector<void*> extra;
   ~Vecs() {
-    for (void* p : ptrs) cudaFreeAsync(p, s);
+    for (void* p : extra) cudaFreeAsync(p, s);
+    if (used > sc.work_cap) {
+      cudaStreamSynchronize(s);  // the solve is over: its vectors are no longer read
+      cudaFree(sc.work);
+      sc.work = nullptr;
+      sc.work_cap = 0;
+      if (cudaMalloc(&sc.work, used) == cudaSuccess) sc.work_cap = used;
+      else sc.work = nullptr;
+    }
   }
   template <class T>
   T* get(long long n) {
+    const size_t bytes = (sizeof(T) * (size_t)(n > 0 ? n : 1) + 16 + 255) / 256 * 256;
+    const size_t off = used;
+    used += bytes;
+    if (sc.work && used <= sc.work_cap) return reinterpret_cast<T*>(static_cast<char*>(sc.work) + off);
     void* p = nullptr;
-    if (cudaMallocAsync(&p, sizeof(T) * (size_t)(n > 0 ? n : 1) + 16, s) != cudaSuccess) return nullptr;
-    ptrs.push_back(p);
+    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) return nullptr;
+    extra.push_back(p);
     return static_cast<T*>(p);
   }
 };
@@ -1423,7 +1451,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
   MB_CUDA_OK(cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned int) * kTicketWords, s));
   if (p.init_x) MB_CUDA_OK(cudaMemsetAsync(d_x, 0, sizeof(double) * n_ext, s));
 
-  Vecs vec{{}, s};
+  Vecs vec{sc, s};
   const int gb = blocks_for(N);
   Plan plan;
   auto t0 = std::chrono::steady_clock::now();
@@ -1944,9 +1972,62 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     for (auto& e : tev) cudaEventDestroy(e);
     if (err != cudaSuccess) return report_cuda(err, "solver loop (timers)", __FILE__, __LINE__);
     for (int k = 0; k < plan.kernels; k++) res.t_kind[plan.kind[k]] += res.kernel_time[k];
+  } else if (!cur.done && p.use_graph && !p.shard && cur.iter == 1 && (p.method != 3 || period <= 400)) {
+    // One graph for the whole solve: a while node whose body is one batch of
+    // iterations followed by loop_continue_kernel, which stops the loop on
+    // the device once the solve has a verdict. The host launches it once and
+    // waits: no host thread in the loop, so a late or descheduled host cannot
+    // leave the GPU idle. With a true-residual interval (FP64), the last
+    // iteration of every body carries the residual kernel: the batch divides
+    // the interval, so every replacement iteration is the last of a body, and
+    // in the other bodies the kernel returns at entry (its flag is raised by
+    // the update kernel of a replacement iteration only). PipeCG's
+    // replacement iteration also recomputes V = A U, which is not gated: its
+    // body is the whole interval. After the verdict the rest of the last body
+    // returns at kernel entry.
+    const int body = p.method == 3 ? period : batch;
+    const int cap = (int)std::min<long long>(iter_cap, 0x7fffffff);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    cudaGraphConditionalHandle handle{};
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t wnode = nullptr;
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = handle;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp);
+    }
+    if (e == cudaSuccess) {
+      cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(s, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int k = 0; k < body; k++) plan.iteration(s, nullptr, period > 0 && k == body - 1);
+        loop_continue_kernel<<<1, 1, 0, s>>>(handle, sc.st, cap);
+        cudaError_t e1 = cudaGetLastError();
+        cudaError_t e2 = cudaStreamEndCapture(s, &bodyg);  // always ended: the stream stays usable
+        e = e1 != cudaSuccess ? e1 : e2;
+      }
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return report_cuda(e, "solver loop (device-side while graph)", __FILE__, __LINE__);
+    SolverState after{};
+    err = read_state(after);
+    if (err != cudaSuccess) return report_cuda(err, "solver loop state", __FILE__, __LINE__);
+    launched_kernels += (long long)after.loops * ((long long)(body - (period > 0 ? 1 : 0)) * kernels_of(false) +
+                                                 (period > 0 ? kernels_of(true) : 0) + 1);
   } else if (!cur.done) {
-    // Two graphs of `batch` iterations: plain, and with the true-residual
-    // kernel in the last iteration (FP64 only).
+    // Host-driven loop (several ranks, a PipeCG interval above 400, or a
+    // solve that does not start at the first iteration): two graphs of
+    // `batch` iterations: plain, and with the true-residual kernel in the last
+    // iteration (FP64 only).
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     const int ngraphs = period > 0 ? 2 : 1;
     if (p.use_graph) {
@@ -1959,16 +2040,25 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         cudaGraphDestroy(graph);
       }
     }
-    // Three launches in flight: the host reads the state word of the oldest
-    // while two more batches keep the GPU busy, so a late host thread (a busy
-    // core) does not leave the device idle. After the verdict the batches
-    // still queued return at kernel entry.
-    constexpr int kInFlight = 3;
-    cudaEvent_t ev[kInFlight];
+    // Several launches in flight: the host reads the state word of the oldest
+    // while the others keep the GPU busy, so a late host thread (a busy core,
+    // a driver query from another process) does not leave the device idle.
+    // The depth is 3 to start with and, once the second launch has been timed,
+    // enough launches to queue about 50 ms of work, at most kMaxInFlight. On
+    // several ranks it stays 3: every rank must enqueue the same number of
+    // launches (they hold collectives), and a timed depth could differ.
+    // After the verdict the batches still queued return at kernel entry (a
+    // few microseconds per kernel).
+    constexpr int kMaxInFlight = 8;
+    int depth = 3;
+    cudaEvent_t ev[kMaxInFlight], t_ev[2];
     for (auto& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (auto& e : t_ev) cudaEventCreate(&e);
     long long next = cur.iter;  // iteration the next enqueued batch starts with (batches start at 1 mod batch)
-    int inflight = 0, slot = 0;
+    int inflight = 0, slot = 0, launched = 0;
+    bool depth_set = p.shard != nullptr;
     while (err == cudaSuccess) {
+      if (launched == 1) cudaEventRecord(t_ev[0], s);
       const int special = is_special(next + batch - 1) ? 1 : 0;
       if (exec[special]) {
         err = cudaGraphLaunch(exec[special], s);
@@ -1979,14 +2069,22 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       if (err != cudaSuccess) break;
       launched_kernels += (long long)(batch - 1) * kernels_of(false) + kernels_of(special);
       next += batch;
+      if (++launched == 2) cudaEventRecord(t_ev[1], s);  // brackets the second launch
       cudaMemcpyAsync(&sc.h_st[slot], sc.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
       cudaEventRecord(ev[slot], s);
-      slot = (slot + 1) % kInFlight;
-      if (++inflight < kInFlight) continue;
-      err = cudaEventSynchronize(ev[slot]);  // the oldest launch (its slot is reused next)
+      slot = (slot + 1) % kMaxInFlight;
+      if (++inflight < depth) continue;
+      const int oldest = (slot + kMaxInFlight - inflight) % kMaxInFlight;
+      err = cudaEventSynchronize(ev[oldest]);
       if (err != cudaSuccess) break;
       inflight--;
-      if (sc.h_st[slot].done) break;
+      if (sc.h_st[oldest].done) break;
+      if (!depth_set && launched >= 2 && cudaEventQuery(t_ev[1]) == cudaSuccess) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t_ev[0], t_ev[1]) == cudaSuccess && ms > 0.f)
+          depth = std::max(3, std::min(kMaxInFlight, (int)std::ceil(50.0 / ms)));
+        depth_set = true;
+      }
       if (next > iter_cap) {
         fprintf(stderr, "** monolis_b200: iteration cap reached without a verdict\n");
         break;
@@ -1995,6 +2093,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     cudaError_t e2 = cudaStreamSynchronize(s);
     if (err == cudaSuccess) err = e2;
     for (auto& e : ev) cudaEventDestroy(e);
+    for (auto& e : t_ev) cudaEventDestroy(e);
     for (auto& e : exec)
       if (e) cudaGraphExecDestroy(e);
     if (err != cudaSuccess) return report_cuda(err, "solver loop", __FILE__, __LINE__);

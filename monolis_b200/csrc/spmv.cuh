@@ -38,14 +38,19 @@ inline SellView<double> view_of<double>(const SellMatrix& m) {
 }
 
 // Column ids of slots k .. k+n-1 (n <= U) of one lane: 32-bit ids (wide
-// slice) or base + lane + 16-bit difference. The branch is uniform over the
-// warp (one slice).
+// slice), base + lane (uniform slice: every difference is zero and the
+// difference stream is not read) or base + lane + 16-bit difference. The
+// branch is uniform over the warp (one slice).
 template <int U>
-__device__ __forceinline__ void load_cols(bool wide, const int* __restrict__ c, const short* __restrict__ c16,
-                                          const int* __restrict__ cb, int lane, int k, int n, int (&j)[U]) {
+__device__ __forceinline__ void load_cols(bool wide, bool uniform, const int* __restrict__ c,
+                                          const short* __restrict__ c16, const int* __restrict__ cb, int lane, int k,
+                                          int n, int (&j)[U]) {
   if (wide) {
 #pragma unroll
     for (int u = 0; u < U; u++) j[u] = u < n ? ld_stream(c + (long long)(k + u) * kSlice) : 0;
+  } else if (uniform) {
+#pragma unroll
+    for (int u = 0; u < U; u++) j[u] = u < n ? __ldg(cb + k + u) + lane : 0;
   } else {
 #pragma unroll
     for (int u = 0; u < U; u++)
@@ -65,8 +70,9 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
   constexpr int B2 = B * B;
   const int lane = row & (kSlice - 1);
   const long long sc = A.slc[row >> 5];
-  const long long base = sc & ~1LL;
+  const long long base = sc & ~3LL;
   const bool wide = !kCols16 || (sc & 1);
+  const bool uni = (sc & 2) != 0;
   const int len = A.rowptr[row + 1] - A.rowptr[row];
   const int* __restrict__ c = A.col + base + lane;
   const short* __restrict__ c16 = A.col16 + base + lane;
@@ -78,7 +84,7 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
   for (; k + U <= len; k += U) {
     int j[U];
     V a[U][B2];
-    load_cols<U>(wide, c, c16, cb, lane, k, U, j);
+    load_cols<U>(wide, uni, c, c16, cb, lane, k, U, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -100,7 +106,7 @@ __device__ __forceinline__ void sell_row_f(const SellView<V>& A, const XF xf, in
   if (U > 1 && rem > 0) {
     int j[U];
     V a[U][B2];
-    load_cols<U>(wide, c, c16, cb, lane, k, rem, j);
+    load_cols<U>(wide, uni, c, c16, cb, lane, k, rem, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -148,11 +154,18 @@ __device__ __forceinline__ short2 ld_stream2(const short2* p) { return __ldcs(p)
 
 // Column ids of slots k .. k+n-1 of a row pair (paired layout).
 template <int U>
-__device__ __forceinline__ void load_cols2(bool wide, const int2* __restrict__ c, const short2* __restrict__ c16,
-                                           const int* __restrict__ cb, int lane2, int k, int n, int2 (&j)[U]) {
+__device__ __forceinline__ void load_cols2(bool wide, bool uniform, const int2* __restrict__ c,
+                                           const short2* __restrict__ c16, const int* __restrict__ cb, int lane2,
+                                           int k, int n, int2 (&j)[U]) {
   if (wide) {
 #pragma unroll
     for (int u = 0; u < U; u++) j[u] = u < n ? ld_stream2(c + (long long)(k + u) * 32) : make_int2(0, 0);
+  } else if (uniform) {
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int b = u < n ? __ldg(cb + k + u) + lane2 : 0;
+      j[u] = make_int2(b, b + 1);
+    }
   } else {
 #pragma unroll
     for (int u = 0; u < U; u++) {
@@ -178,8 +191,9 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   const int r0 = 2 * t;
   const int lane2 = 2 * (t & 31);
   const long long sc = A.slc2[t >> 5];
-  const long long base = sc & ~1LL;
+  const long long base = sc & ~3LL;
   const bool wide = !kCols16 || (sc & 1);
+  const bool uni = (sc & 2) != 0;
   const int len0 = A.rowptr[r0 + 1] - A.rowptr[r0];
   const int len1 = (r0 + 1 < A.N) ? A.rowptr[r0 + 2] - A.rowptr[r0 + 1] : 0;
   const int len = len0 > len1 ? len0 : len1;
@@ -193,7 +207,7 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   for (; k + U <= len; k += U) {
     int2 j[U];
     float2 a[U][B2];
-    load_cols2<U>(wide, c, c16, cb, lane2, k, U, j);
+    load_cols2<U>(wide, uni, c, c16, cb, lane2, k, U, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll
@@ -220,7 +234,7 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   if (rem > 0) {
     int2 j[U];
     float2 a[U][B2];
-    load_cols2<U>(wide, c, c16, cb, lane2, k, rem, j);
+    load_cols2<U>(wide, uni, c, c16, cb, lane2, k, rem, j);
 #pragma unroll
     for (int u = 0; u < U; u++)
 #pragma unroll

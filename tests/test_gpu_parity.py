@@ -128,16 +128,37 @@ def test_spmv_mixed_wide_and_compressed_slices(gpu, oracle, n, n_far):
 def test_spmv_structured_grid_compresses(gpu, oracle):
     """192^3 7-point grid: the rows at both ends of a grid line put stencil
     neighbours +-n and +-n^2 into one slot; with the midpoint base every
-    slice still compresses, and the FP64 SpMV stays bit-identical."""
-    mp, b = build(gpu, "convection_diffusion", n=192, peclet=5.0)
-    mo, _ = build(oracle, "convection_diffusion", n=192, peclet=5.0)
+    slice still compresses. The slices inside a grid line have every block
+    at the same offset from its row: they are uniform and read no column
+    stream (4 of the 6 32-row slices of a line, 1 of the 3 64-row ones). The
+    FP64 SpMV stays bit-identical, the FP32 one within its rounding bound."""
+    import torch
+    n = 192
+    mp, b = build(gpu, "convection_diffusion", n=n, peclet=5.0)
+    mo, _ = build(oracle, "convection_diffusion", n=n, peclet=5.0)
     mp.set_matrix_cache(True)
     mp.set_precision(1)
     mp.device_prepare()
     assert mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP64] == 0
     assert mp.Iarray[api.B200_PRM_I_WIDE_SLICES_FP32] == 0
+    assert mp.Iarray[api.B200_PRM_I_UNIFORM_SLICES_FP64] == n * n * 4
+    assert mp.Iarray[api.B200_PRM_I_UNIFORM_SLICES_FP32] == n * n * 1
+    nz = int(mo.csr_index()[-1])
+    # the layout's bytes: no difference stream in the uniform slices
+    assert mp.Rarray[api.B200_PRM_R_SPMV_BYTES_FP64] < nz * (8 + 2) + (n ** 3 + 1) * 4 + 2 * n ** 3 * 8
     x = np.random.default_rng(4).standard_normal(len(b))
     assert bits_equal(mp.matvec(x), mo.matvec(x))
+    x32 = x.astype(np.float32)
+    vals32 = mo.values().astype(np.float32).astype(np.float64)
+    mo.values()[:] = np.abs(vals32)
+    bound = mo.matvec(np.abs(x32.astype(np.float64)))
+    mo.values()[:] = vals32
+    y_ref = mo.matvec(x32.astype(np.float64))
+    d_x = torch.from_numpy(x32).cuda()
+    d_y = torch.empty_like(d_x)
+    mp.device_matvec(d_x.data_ptr(), d_y.data_ptr(), fp32=True)
+    torch.cuda.synchronize()
+    assert np.all(np.abs(d_y.cpu().numpy().astype(np.float64) - y_ref) <= 1e-6 * bound + 1e-30)
 
 
 def test_spmv_ndof2_random_blocks(gpu, oracle):
