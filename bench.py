@@ -183,6 +183,36 @@ def kernel_times(m, stream, d_b, d_x):
     return [m.Rarray[api.B200_PRM_R_TIME_KERNEL + k] / it for k in range(8)], it
 
 
+def workload_c1(lib, args):
+    """The reference's CPU-runnable configuration: 3D 7-point Laplacian 32^3,
+    CG + DIAG to 1e-8, FP64 and FP32-refined, device-resident b and x (five
+    timed solves after one untimed)."""
+    import torch
+    m = api.Monolis(lib)
+    b = problems.laplacian(m, n=32)
+    m.quiet()
+    m.set_error_abort(False)
+    m.set_method(api.ITER_CG)
+    m.set_precond(api.PREC_DIAG)
+    m.set_tolerance(TOL)
+    m.set_maxiter(10000)
+    m.set_matrix_cache(True)
+    stream = torch.cuda.ExternalStream(api.stream_handle(lib))
+    d_b = torch.from_numpy(b).cuda()
+    d_x = torch.zeros_like(d_b)
+    out = {"workload": "3D 7-point Laplacian 32^3 (32,768 unknowns), CG + DIAG, rel.res 1e-8",
+           "oracle_iterations": fixture().get("laplacian_n32_cg_diag_tol1e-08")}
+    for prec, name in ((0, "fp64"), (1, "mixed")):
+        m.set_precision(prec)
+        m.device_prepare()
+        device_solve_timed(m, stream, d_b, d_x)
+        ts = [device_solve_timed(m, stream, d_b, d_x) for _ in range(5)]
+        out[name] = {"s": float(np.median(ts)), "s_each": ts, "iterations": m.get_converge_iter(),
+                     "rel_residual": m.get_converge_residual()}
+    m.finalize()
+    return out
+
+
 def workload_c3(lib, args, peak):
     """Nonsymmetric 7-point upwind convection-diffusion, 256^3 unknowns,
     BiCGSTAB + DIAG to 1e-8: FP64 and FP32-refined, three cell Peclet numbers."""
@@ -789,8 +819,8 @@ def main():
     ap.add_argument("--cpu-baseline-iters", type=int, default=200,
                     help="iterations of the CPU-baseline sample in our arm (about 10-30 s on the host)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workloads", default="c3,c4,c5",
-                    help="secondary workloads to run after the headline (any of c3,c4,c5, or none)")
+    ap.add_argument("--workloads", default="c1,c3,c4,c5",
+                    help="secondary workloads to run after the headline (any of c1,c3,c4,c5, or none)")
     ap.add_argument("--replicas", action="store_true",
                     help="with N > 1: N independent copies of the headline system (weak scaling) instead of "
                          "the row-partitioned solve of one system")
@@ -1091,7 +1121,9 @@ def main_ours(args, world, rank, local):
     if rank == 0 and world == 1:
         for w in [w for w in args.workloads.split(",") if w and w != "none"]:
             try:
-                if w == "c3":
+                if w == "c1":
+                    workloads["c1"] = workload_c1(lib, args)
+                elif w == "c3":
                     workloads["c3"] = workload_c3(lib, args, peak)
                 elif w == "c5":
                     workloads["c5"] = workload_c5(lib, args)

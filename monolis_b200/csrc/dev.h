@@ -115,6 +115,7 @@ struct Scratch {
   size_t partials_cap = 0;
   void* work = nullptr;           // work vectors of the solves (grows to the largest solve's need)
   size_t work_cap = 0;
+  int solves = 0;                 // solves that needed more than the arena (the first one does not grow it)
 };
 
 // ---- matrix build on the device ----

@@ -1347,7 +1347,8 @@ __global__ void mixed_fold_kernel(long long n, double* __restrict__ x, float* __
 // Work vectors of one solve, carved in order from the scratch's work arena
 // (kept between solves, so a repeated solve maps no new memory). Vectors
 // past the arena's end are allocated from the stream's pool and freed after
-// the solve; the arena then grows to the whole solve's need for the next one.
+// the solve; from the second solve of a struct on, the arena then grows to
+// the whole solve's need for the next one (a struct solved once keeps none).
 struct Vecs {
   Scratch& sc;
   cudaStream_t s;
@@ -1355,7 +1356,7 @@ struct Vecs {
   std::vector<void*> extra;
   ~Vecs() {
     for (void* p : extra) cudaFreeAsync(p, s);
-    if (used > sc.work_cap) {
+    if (used > sc.work_cap && sc.solves++ > 0) {
       cudaStreamSynchronize(s);  // the solve is over: its vectors are no longer read
       cudaFree(sc.work);
       sc.work = nullptr;
