@@ -146,14 +146,35 @@ template <int B, int U>
 __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsize, int grank,
                                              const cg::cluster_group& cl, GroupShared& sh) {
   const BatchSys S = a.sys[si];
+  // this CTA's rows: a multiple of 4 (a system has a multiple of 64), so the
+  // vector phases can move whole 16-byte groups of R rows (RowGroup)
   const long long pair0 = S.row0 / 2, npairs = S.nrows / 2;
-  const long long chunk = (npairs + gsize - 1) / gsize;
+  const long long chunk = 2 * ((npairs / 2 + gsize - 1) / gsize);
   const long long plo = pair0 + min(npairs, chunk * grank);
   const long long phi = pair0 + min(npairs, chunk * (grank + 1));
   const long long rlo = 2 * plo, rhi = 2 * phi;  // this CTA's block rows
   const long long elo = rlo * B, ehi = rhi * B;  // and vector entries
   const int tid = threadIdx.x, nt = blockDim.x;
   int ph = 0;
+  using RG = RowGroup<float, B>;
+  constexpr int R = RG::R, E = RG::E;
+  const long long g0 = rlo / R, g1 = rhi / R;
+  const bool alu_vec = (a.N % R) == 0;
+  // f(k-groups, first group) over this CTA's groups g0 + tid, g0 + tid + nt,
+  // ..., Kc groups a step (each thread then has Kc 16-byte loads of every
+  // operand in flight)
+  auto for_groups = [&](auto Kc, auto&& f) {
+    constexpr int K = decltype(Kc)::value;
+    long long g = g0 + tid;
+    if constexpr (K > 1)
+      for (; g + (long long)(K - 1) * nt < g1; g += (long long)K * nt) f(Kc, g);
+    for (; g < g1; g += nt) f(std::integral_constant<int, 1>{}, g);
+  };
+  // ndof 1: the vector phases move 16-byte groups of 4 rows, two groups a
+  // step for the p update. Larger blocks keep one entry a thread a step: their
+  // groups (and DIAG blocks) do not fit the register budget of 2 CTAs of 512
+  // threads per SM.
+  constexpr int KP = 2;
 
   for (long long i = elo + tid; i < ehi; i += nt) {
     a.x[i] = 0.0;
@@ -199,11 +220,47 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
       // P = Z + beta P (P = Z first); fold Y into X after a refresh
       const bool first = iter == 1;
       const float fb = (float)beta;
-      for (long long i = elo + tid; i < ehi; i += nt) {
-        a.p[i] = first ? a.z[i] : fmaf(fb, a.p[i], a.z[i]);
-        if (fold) {
-          a.x[i] += (double)a.y[i];
-          a.y[i] = 0.0f;
+      if constexpr (B == 1) {
+        for_groups(std::integral_constant<int, KP>{}, [&](auto Kc, long long g) {
+          constexpr int KK = decltype(Kc)::value;
+          float zv[KK][E], pv[KK][E];
+#pragma unroll
+          for (int k = 0; k < KK; k++) {
+            const long long e0 = (g + (long long)k * nt) * E;
+            vload<float, E>(a.z + e0, zv[k]);
+            if (!first) vload<float, E>(a.p + e0, pv[k]);
+          }
+#pragma unroll
+          for (int k = 0; k < KK; k++) {
+#pragma unroll
+            for (int e = 0; e < E; e++) pv[k][e] = first ? zv[k][e] : fmaf(fb, pv[k][e], zv[k][e]);
+            vstore<float, E>(a.p + (g + (long long)k * nt) * E, pv[k]);
+          }
+          if (fold) {
+#pragma unroll
+            for (int k = 0; k < KK; k++) {
+              const long long e0 = (g + (long long)k * nt) * E;
+              double xv[E];
+              float yv[E];
+              vload<double, E>(a.x + e0, xv);
+              vload<float, E>(a.y + e0, yv);
+#pragma unroll
+              for (int e = 0; e < E; e++) {
+                xv[e] += (double)yv[e];
+                yv[e] = 0.0f;
+              }
+              vstore<double, E>(a.x + e0, xv);
+              vstore<float, E>(a.y + e0, yv);
+            }
+          }
+        });
+      } else {
+        for (long long i = elo + tid; i < ehi; i += nt) {
+          a.p[i] = first ? a.z[i] : fmaf(fb, a.p[i], a.z[i]);
+          if (fold) {
+            a.x[i] += (double)a.y[i];
+            a.y[i] = 0.0f;
+          }
         }
       }
       fold = false;
@@ -230,22 +287,57 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
       const float fa = (float)alpha;
       // Y += alpha P, R -= alpha Q, Z = M^-1 R, <R,R>, <R,Z>
       v[0] = v[1] = 0.0;
-      for (long long row = rlo + tid; row < rhi; row += nt) {
-        float t[B], zz[B];
+      if constexpr (B == 1) {
+        for_groups(std::integral_constant<int, 1>{}, [&](auto Kc, long long g) {
+          constexpr int KK = decltype(Kc)::value;
+          float pv[KK][E], qv[KK][E], rv[KK][E], yv[KK][E];
 #pragma unroll
-        for (int c = 0; c < B; c++) {
-          const long long i = row * B + c;
-          a.y[i] = fmaf(fa, a.p[i], a.y[i]);
-          t[c] = fmaf(-fa, a.q[i], a.r[i]);
-          a.r[i] = t[c];
-          zz[c] = t[c];
-        }
-        if (a.prec) diag_row<B, float>(a.alu32, a.N, (int)row, zz);
+          for (int k = 0; k < KK; k++) {
+            const long long e0 = (g + (long long)k * nt) * E;
+            vload<float, E>(a.p + e0, pv[k]);
+            vload<float, E>(a.q + e0, qv[k]);
+            vload<float, E>(a.r + e0, rv[k]);
+            vload<float, E>(a.y + e0, yv[k]);
+          }
 #pragma unroll
-        for (int c = 0; c < B; c++) {
-          a.z[row * B + c] = zz[c];
-          v[0] += (double)t[c] * (double)t[c];
-          v[1] += (double)t[c] * (double)zz[c];
+          for (int k = 0; k < KK; k++) {
+            const long long gk = g + (long long)k * nt, e0 = gk * E;
+            float zz[E];
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+              yv[k][e] = fmaf(fa, pv[k][e], yv[k][e]);
+              rv[k][e] = fmaf(-fa, qv[k][e], rv[k][e]);
+              zz[e] = rv[k][e];
+            }
+            vstore<float, E>(a.y + e0, yv[k]);
+            vstore<float, E>(a.r + e0, rv[k]);
+            if (a.prec) diag_rows<B, float, R>(a.alu32, a.N, gk * R, alu_vec, zz);
+            vstore<float, E>(a.z + e0, zz);
+#pragma unroll
+            for (int e = 0; e < E; e++) {
+              v[0] += (double)rv[k][e] * (double)rv[k][e];
+              v[1] += (double)rv[k][e] * (double)zz[e];
+            }
+          }
+        });
+      } else {
+        for (long long row = rlo + tid; row < rhi; row += nt) {
+          float t[B], zz[B];
+#pragma unroll
+          for (int c = 0; c < B; c++) {
+            const long long i = row * B + c;
+            a.y[i] = fmaf(fa, a.p[i], a.y[i]);
+            t[c] = fmaf(-fa, a.q[i], a.r[i]);
+            a.r[i] = t[c];
+            zz[c] = t[c];
+          }
+          if (a.prec) diag_row<B, float>(a.alu32, a.N, (int)row, zz);
+#pragma unroll
+          for (int c = 0; c < B; c++) {
+            a.z[row * B + c] = zz[c];
+            v[0] += (double)t[c] * (double)t[c];
+            v[1] += (double)t[c] * (double)zz[c];
+          }
         }
       }
       group_sum<2>(v, sh, cl, gsize, ph);

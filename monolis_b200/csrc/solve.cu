@@ -659,23 +659,6 @@ __global__ void shard_grop_kernel(SolverState* st, double* hist) {
 // ---------------------------------------------------------------------------
 // BiCGSTAB kernels (src/iterative/BiCGSTAB.f90:87-170)
 // ---------------------------------------------------------------------------
-// Per-row DIAG apply of E = R*B values held in registers (R rows of B).
-template <int B, class T, int R>
-__device__ __forceinline__ void diag_rows(const T* __restrict__ alu, int N, long long row0, bool alu_vec,
-                                          T (&w)[R * B]) {
-  T L[B * B][R];
-  load_alu_rows<T, B, R>(alu, N, row0, alu_vec, L);
-#pragma unroll
-  for (int k = 0; k < R; k++) {
-    T t[B];
-#pragma unroll
-    for (int c = 0; c < B; c++) t[c] = w[k * B + c];
-    diag_solve<B, T>([&](int j, int kk) { return L[j * B + kk][k]; }, t);
-#pragma unroll
-    for (int c = 0; c < B; c++) w[k * B + c] = t[c];
-  }
-}
-
 // P = R + beta*(P - omega*V) (or P = R on iteration 1); PT = M^-1 P.
 // Mixed precision (x64 != null): after a refresh it also folds the FP32
 // correction into the FP64 solution, X += Y, Y = 0. Register-blocked like

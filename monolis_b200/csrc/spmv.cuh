@@ -368,6 +368,23 @@ __device__ __forceinline__ void diag_row(const T* __restrict__ alu, int N, int r
   diag_solve<B, T>([&](int j, int k) { return alu[(long long)(j * B + k) * N + row]; }, t);
 }
 
+// Per-row DIAG apply of E = R*B values held in registers (R rows of B).
+template <int B, class T, int R>
+__device__ __forceinline__ void diag_rows(const T* __restrict__ alu, int N, long long row0, bool alu_vec,
+                                          T (&w)[R * B]) {
+  T L[B * B][R];
+  load_alu_rows<T, B, R>(alu, N, row0, alu_vec, L);
+#pragma unroll
+  for (int k = 0; k < R; k++) {
+    T t[B];
+#pragma unroll
+    for (int c = 0; c < B; c++) t[c] = w[k * B + c];
+    diag_solve<B, T>([&](int j, int kk) { return L[j * B + kk][k]; }, t);
+#pragma unroll
+    for (int c = 0; c < B; c++) w[k * B + c] = t[c];
+  }
+}
+
 // Resident blocks of 256 threads per SM that the SpMV kernels are compiled
 // for. With 1x1 blocks a row has few slots and the kernels are bound by
 // memory latency, not bandwidth: at 256^3 (7 entries a row) six blocks per
