@@ -171,9 +171,9 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
     for (; g < g1; g += nt) f(std::integral_constant<int, 1>{}, g);
   };
   // ndof 1: the vector phases move 16-byte groups of 4 rows, two groups a
-  // step for the p update. Larger blocks keep one entry a thread a step: their
-  // groups (and DIAG blocks) do not fit the register budget of 2 CTAs of 512
-  // threads per SM.
+  // step. Larger blocks keep one entry a thread a step: their groups (and
+  // DIAG blocks) do not fit the register budget of 2 CTAs of 512 threads per
+  // SM.
   constexpr int KP = 2;
 
   for (long long i = elo + tid; i < ehi; i += nt) {
@@ -288,7 +288,7 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
       // Y += alpha P, R -= alpha Q, Z = M^-1 R, <R,R>, <R,Z>
       v[0] = v[1] = 0.0;
       if constexpr (B == 1) {
-        for_groups(std::integral_constant<int, 1>{}, [&](auto Kc, long long g) {
+        for_groups(std::integral_constant<int, KP>{}, [&](auto Kc, long long g) {
           constexpr int KK = decltype(Kc)::value;
           float pv[KK][E], qv[KK][E], rv[KK][E], yv[KK][E];
 #pragma unroll
