@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256, SpmvMinBlocks<B>::value) spmv_kernel(Sell
 }
 
 template <int B, int U>
-__global__ void __launch_bounds__(256, SpmvMinBlocks<B>::value) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
+__global__ void __launch_bounds__(256, SpmvMinBlocks2<B>::value) spmv2_kernel(SellView2 A, const float* __restrict__ x, float* __restrict__ y) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; 2 * t < A.N; t += gridDim.x * blockDim.x) {
     float y0[B], y1[B];
     sell_row2<B, U>(A, x, t, y0, y1);

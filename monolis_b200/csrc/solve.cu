@@ -959,7 +959,7 @@ __device__ void fin_mixed_bicg(SolverState* st, double rr, double rrt, double* h
 
 // V = A PT (FP32 paired layout); c2 = <RT,V>; alpha = rho/c2.
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks2<B>::value)
     mbicg_v_kernel(SellView2 A, const float* __restrict__ pt, float* __restrict__ vv, const float* __restrict__ rt,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
@@ -991,7 +991,7 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
 
 // T = A ST (FP32 paired layout); (T,S), (T,T); omega.
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks2<B>::value)
     mbicg_t_kernel(SellView2 A, const float* __restrict__ stv, float* __restrict__ t, const float* __restrict__ s,
                    double* partials, unsigned int* ticket, SolverState* st) {
   if (st->done) return;
@@ -1080,7 +1080,7 @@ __global__ void mixed_p_kernel(long long n, float* __restrict__ p, const float* 
 
 // FP32 paired-layout SpMV fused with <P,Q> (mixed precision inner loop).
 template <int B, int U>
-__global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
+__global__ void __launch_bounds__(kThreads, SpmvMinBlocks2<B>::value)
     cg_spmv2_kernel(SellView2 A, const float* __restrict__ p, float* __restrict__ q, double* partials,
                     unsigned int* ticket, SolverState* st) {
   if (st->done) return;

@@ -395,6 +395,15 @@ template <int B>
 struct SpmvMinBlocks {
   static constexpr int value = B == 1 ? 6 : 1;
 };
+// The same for the FP32 kernels of the paired layout, where a thread carries
+// two rows: at 1x1 blocks five resident blocks (48 registers, no spills)
+// beat six (40, about 100 bytes of spills a thread at 8 slots in flight) in
+// BiCGSTAB at 256^3: V = A PT 172 -> 167 us, T = A ST 177 -> 168 us; four
+// (64 registers) were slower (184 us).
+template <int B>
+struct SpmvMinBlocks2 {
+  static constexpr int value = B == 1 ? 5 : 1;
+};
 
 // Compile-time block size and unroll depth from their runtime values.
 template <class F>
