@@ -56,7 +56,7 @@ static const int MONOLIS_B200_PRM_I_UNIFORM_SLICES_FP32 = 47; /* out: same for t
 
 static const int MONOLIS_B200_PRM_R_REFRESH_DELTA  = 30; /* mixed precision: FP64 refresh when ||r|| has dropped
                                                             below delta * its largest value since the last one
-                                                            (0: 0.1 for CG, 0.01 for BiCGSTAB) */
+                                                            (0: 0.1 for CG, 0.2 for BiCGSTAB) */
 static const int MONOLIS_B200_PRM_R_TIME_H2D       = 31; /* out: seconds spent on host->device copies */
 static const int MONOLIS_B200_PRM_R_TIME_D2H       = 32; /* out: seconds spent on device->host copies */
 static const int MONOLIS_B200_PRM_R_TIME_LOOP      = 33; /* out: seconds in the device iteration loop */
