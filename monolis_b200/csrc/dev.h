@@ -113,9 +113,6 @@ struct Scratch {
   double* hist = nullptr;         // residual history (max_iter + 1)
   size_t hist_cap = 0;
   size_t partials_cap = 0;
-  void* work = nullptr;           // work vectors of the solves (grows to the largest solve's need)
-  size_t work_cap = 0;
-  int solves = 0;                 // solves that needed more than the arena (the first one does not grow it)
 };
 
 // ---- matrix build on the device ----

@@ -608,7 +608,6 @@ int scratch_ensure(Scratch& sc, size_t hist_len) {
 }
 
 void scratch_free(Scratch& sc) {
-  cudaFree(sc.work);
   cudaFree(sc.partials);
   cudaFree(sc.ticket);
   cudaFree(sc.st);

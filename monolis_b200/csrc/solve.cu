@@ -1327,35 +1327,55 @@ __global__ void mixed_fold_kernel(long long n, double* __restrict__ x, float* __
 // ---------------------------------------------------------------------------
 
 
-// Work vectors of one solve, carved in order from the scratch's work arena
-// (kept between solves, so a repeated solve maps no new memory). Vectors
-// past the arena's end are allocated from the stream's pool and freed after
-// the solve; from the second solve of a struct on, the arena then grows to
-// the whole solve's need for the next one (a struct solved once keeps none).
+// Per-device stream-ordered pool for the solvers' work vectors, owned by the
+// library. Its release threshold is unlimited: memory a solve frees stays
+// mapped in the pool, and the next solve (of this struct or any other) takes
+// it back without mapping pages again (the default pool returns freed memory
+// to the driver at every synchronisation, and re-mapping a gigabyte of
+// vectors cost milliseconds per solve). Null if it cannot be made (the
+// stream's default pool is used then).
+cudaMemPool_t work_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  static bool failed[64] = {};
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[d] && !failed[d]) {
+    cudaMemPoolProps pr = {};
+    pr.allocType = cudaMemAllocationTypePinned;
+    pr.handleTypes = cudaMemHandleTypeNone;
+    pr.location.type = cudaMemLocationTypeDevice;
+    pr.location.id = d;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &pr) != cudaSuccess) {
+      failed[d] = true;
+      cudaGetLastError();
+      return nullptr;
+    }
+    unsigned long long thr = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
+    pools[d] = p;
+  }
+  return pools[d];
+}
+
+// Work vectors of one solve, from the work pool, freed (back to the pool)
+// after the solve.
 struct Vecs {
   Scratch& sc;
   cudaStream_t s;
-  size_t used = 0;
   std::vector<void*> extra;
   ~Vecs() {
     for (void* p : extra) cudaFreeAsync(p, s);
-    if (used > sc.work_cap && sc.solves++ > 0) {
-      cudaStreamSynchronize(s);  // the solve is over: its vectors are no longer read
-      cudaFree(sc.work);
-      sc.work = nullptr;
-      sc.work_cap = 0;
-      if (cudaMalloc(&sc.work, used) == cudaSuccess) sc.work_cap = used;
-      else sc.work = nullptr;
-    }
   }
   template <class T>
   T* get(long long n) {
     const size_t bytes = (sizeof(T) * (size_t)(n > 0 ? n : 1) + 16 + 255) / 256 * 256;
-    const size_t off = used;
-    used += bytes;
-    if (sc.work && used <= sc.work_cap) return reinterpret_cast<T*>(static_cast<char*>(sc.work) + off);
     void* p = nullptr;
-    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) return nullptr;
+    cudaMemPool_t pool = work_pool();
+    if ((pool ? cudaMallocFromPoolAsync(&p, bytes, pool, s) : cudaMallocAsync(&p, bytes, s)) != cudaSuccess)
+      return nullptr;
     extra.push_back(p);
     return static_cast<T*>(p);
   }
