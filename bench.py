@@ -496,12 +496,13 @@ def multi_rhs_run(lib, sysm, rhs):
         X = d_X.cpu().numpy()
         true = [float(np.linalg.norm(b - problems.csr_matvec(ix, it, v, X[k])) / np.linalg.norm(b))
                 for k, b in enumerate(rhs)]
-        # roofline: per iteration the matrix once (values + 32-bit column ids + offsets, in the loop
-        # precision) while any right-hand side is active, and 12 vector passes plus the DIAG factors
-        # per active right-hand side; FP64 refreshes not counted
+        # roofline: per iteration the matrix and the DIAG factors once (values + 32-bit column ids +
+        # offsets, in the loop precision) while any right-hand side is active, and 11 vector passes per
+        # active right-hand side (product: z, p read, p, q written; update: p, q, r, y read, y, r, z
+        # written); FP64 refreshes not counted
         peak, _ = measured_peak()
         sv = 4 if prec == 1 else 8
-        byts = int(its.max()) * (len(it) * (sv + 4) + (n + 1) * 4) + float(its.sum()) * 13 * n * sv
+        byts = int(its.max()) * (len(it) * (sv + 4) + (n + 1) * 4 + n * sv) + float(its.sum()) * 11 * n * sv
         out[name] = {"s": times[-1], "all_converged": bool(np.all(st == 0)), "max_true_rel_residual": max(true),
                      "iterations_max": int(its.max()), "iterations_mean": float(its.mean()),
                      "roofline": {"bound": "hbm", "loop_bytes": float(byts), "achieved_gbs": byts / times[-1] / 1e9,

@@ -537,6 +537,9 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
 #pragma unroll
       for (int j = 0; j < 4; j++) alpha[j] = lv[j] ? (T)__ldcg(&c->alpha[4 * qd + j]) : T(0);
       double v0[4] = {0.0, 0.0, 0.0, 0.0}, v1[4] = {0.0, 0.0, 0.0, 0.0};
+      // z is rewritten for the live right-hand sides; it is read only to keep
+      // a stopped one's entries when this thread has one
+      const bool keep_z = !(lv[0] && lv[1] && lv[2] && lv[3]);
       for (long long rb = wrow0; anyl && rb < N; rb += sweep) {
         const long long row = rb + g;
         if (row >= N) continue;
@@ -544,12 +547,12 @@ __global__ void __launch_bounds__(kMultiThreads, B <= 2 ? (sizeof(T) == 4 ? 4 : 
 #pragma unroll
         for (int cc = 0; cc < B; cc++) {
           const long long i = at(row, cc);
-          T p4[4], q4[4], r4[4], y4[4], z4[4];
+          T p4[4], q4[4], r4[4], y4[4], z4[4] = {T(0), T(0), T(0), T(0)};
           ld4<false>(pnew + i, p4);
           ld4<false>(qv + i, q4);
           ld4<false>(rv + i, r4);
           ld4<false>(yv + i, y4);
-          ld4<false>(zv + i, z4);
+          if (keep_z) ld4<false>(zv + i, z4);
 #pragma unroll
           for (int j = 0; j < 4; j++) {
             y4[j] = lv[j] ? fmat<T>(alpha[j], p4[j], y4[j]) : y4[j];
