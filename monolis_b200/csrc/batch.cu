@@ -267,15 +267,34 @@ __device__ __forceinline__ void solve_system(const BatchArgs a, int si, int gsiz
       group_sync(cl, gsize);
       // Q = A P (FP32), <P,Q>
       double w[1] = {0.0};
-      for (long long t = plo + tid; t < phi; t += nt) {
-        float q0[B], q1[B];
-        sell_row2<B, U, true, kBatchCols16>(a.A32, a.p, (int)t, q0, q1);
+      if constexpr (B == 1) {
+        // two row pairs a step, both pairs' loads in flight (sell_row2_two)
+        auto xf = [&](long long i) { return ldx<true>(a.p + i); };
+        for (long long t = plo + tid; t < phi; t += 2 * (long long)nt) {
+          const long long tb = t + nt;
+          const bool hb = tb < phi;
+          float qa[2], qb[2];
+          sell_row2_two<U, kBatchCols16>(a.A32, xf, (int)t, (int)(hb ? tb : t), hb, qa, qb);
+          a.q[2 * t] = qa[0];
+          a.q[2 * t + 1] = qa[1];
+          w[0] += (double)a.p[2 * t] * (double)qa[0] + (double)a.p[2 * t + 1] * (double)qa[1];
+          if (hb) {
+            a.q[2 * tb] = qb[0];
+            a.q[2 * tb + 1] = qb[1];
+            w[0] += (double)a.p[2 * tb] * (double)qb[0] + (double)a.p[2 * tb + 1] * (double)qb[1];
+          }
+        }
+      } else {
+        for (long long t = plo + tid; t < phi; t += nt) {
+          float q0[B], q1[B];
+          sell_row2<B, U, true, kBatchCols16>(a.A32, a.p, (int)t, q0, q1);
 #pragma unroll
-        for (int c = 0; c < B; c++) {
-          const long long i0 = 2 * t * B + c, i1 = (2 * t + 1) * B + c;
-          a.q[i0] = q0[c];
-          a.q[i1] = q1[c];
-          w[0] += (double)a.p[i0] * (double)q0[c] + (double)a.p[i1] * (double)q1[c];
+          for (int c = 0; c < B; c++) {
+            const long long i0 = 2 * t * B + c, i1 = (2 * t + 1) * B + c;
+            a.q[i0] = q0[c];
+            a.q[i1] = q1[c];
+            w[0] += (double)a.p[i0] * (double)q0[c] + (double)a.p[i1] * (double)q1[c];
+          }
         }
       }
       group_sum<1>(w, sh, cl, gsize, ph);

@@ -262,6 +262,73 @@ __device__ __forceinline__ void sell_row2_f(const SellView2& A, const XF xf, int
   }
 }
 
+// Two row pairs of the paired layout at once (1x1 blocks): pairs ta and tb
+// (tb skipped when !hb) advance slot by slot together, U slots of each in
+// flight, so a thread keeps both pairs' loads in flight at once. Each row
+// adds its slots in the order of sell_row2_f, with the same results.
+template <int U, bool kCols16, class XF>
+__device__ __forceinline__ void sell_row2_two(const SellView2& A, const XF xf, int ta, int tb, bool hb,
+                                              float (&ya)[2], float (&yb)[2]) {
+  const int tt[2] = {ta, tb};
+  const int2* __restrict__ c[2];
+  const short2* __restrict__ c16[2];
+  const int* __restrict__ cb[2];
+  const float2* __restrict__ v[2];
+  bool wide[2], uni[2];
+  int len[2], lane2[2];
+#pragma unroll
+  for (int p = 0; p < 2; p++) {
+    const int t = tt[p];
+    const long long sc = A.slc2[t >> 5];
+    const long long base = sc & ~3LL;
+    wide[p] = !kCols16 || (sc & 1);
+    uni[p] = (sc & 2) != 0;
+    lane2[p] = 2 * (t & 31);
+    const int r0 = 2 * t;
+    const int l0 = A.rowptr[r0 + 1] - A.rowptr[r0];
+    const int l1 = (r0 + 1 < A.N) ? A.rowptr[r0 + 2] - A.rowptr[r0 + 1] : 0;
+    len[p] = (p == 0 || hb) ? (l0 > l1 ? l0 : l1) : 0;
+    c[p] = reinterpret_cast<const int2*>(A.col2 + base + lane2[p]);
+    c16[p] = reinterpret_cast<const short2*>(A.col16p + base + lane2[p]);
+    cb[p] = A.cbase2 + (base >> 6);
+    v[p] = reinterpret_cast<const float2*>(A.val + base + lane2[p]);
+  }
+  float y[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+  const int lmax = len[0] > len[1] ? len[0] : len[1];
+  for (int k = 0; k < lmax; k += U) {
+    int2 j[2][U];
+    float2 a[2][U];
+    float x0[2][U], x1[2][U];
+#pragma unroll
+    for (int p = 0; p < 2; p++) {
+      const int n = len[p] - k;
+      load_cols2<U>(wide[p], uni[p], c[p], c16[p], cb[p], lane2[p], k, n, j[p]);
+#pragma unroll
+      for (int u = 0; u < U; u++) a[p][u] = u < n ? ld_stream2(v[p] + (long long)(k + u) * 32) : make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const bool in = u < len[p] - k;
+        x0[p][u] = in ? xf((long long)j[p][u].x) : 0.f;
+        x1[p][u] = in ? xf((long long)j[p][u].y) : 0.f;
+      }
+#pragma unroll
+    for (int p = 0; p < 2; p++)
+#pragma unroll
+      for (int u = 0; u < U; u++)
+        if (u < len[p] - k) {
+          y[p][0] = fmaf(a[p][u].x, x0[p][u], y[p][0]);
+          y[p][1] = fmaf(a[p][u].y, x1[p][u], y[p][1]);
+        }
+  }
+  ya[0] = y[0][0];
+  ya[1] = y[0][1];
+  yb[0] = y[1][0];
+  yb[1] = y[1][1];
+}
+
 template <int B, int U, bool kCoherent = false, bool kCols16 = true>
 __device__ __forceinline__ void sell_row2(const SellView2& A, const float* __restrict__ x, int t, float (&y0)[B],
                                           float (&y1)[B]) {
