@@ -782,10 +782,12 @@ def timed_device_solves(m, stream, d_b, d_x, precision, warmup, steps, clock_ind
     return times, iters, launches, (sampler.summary() if sampler else None)
 
 
-def e2e_calls(m, b, n_unk, precision, calls):
+def e2e_calls(m, b, n_unk, precision, calls, parts=None):
     """monolis_solve_R with pinned host b and x, matrix uploaded by every
     call (the library's default, like the reference's GPU build); one
-    untimed call first. Returns the per-call wall seconds."""
+    untimed call first. Returns the per-call wall seconds; `parts` (a list)
+    receives each timed call's split as the library reports it: host->device
+    copies (matrix and b), the device loop, the device->host copy of x."""
     import torch
     hb = torch.from_numpy(b).pin_memory()
     hx = torch.zeros(n_unk, dtype=torch.float64).pin_memory()
@@ -801,6 +803,11 @@ def e2e_calls(m, b, n_unk, precision, calls):
             raise RuntimeError(f"monolis_solve_R failed: status {m.get_error_tag()}")
         if k >= 1:
             out.append(dt)
+            if parts is not None:
+                R = m.Rarray
+                parts.append({"wall_s": round(dt, 4), "h2d_s": round(R[api.B200_PRM_R_TIME_H2D], 4),
+                              "loop_s": round(R[api.B200_PRM_R_TIME_LOOP], 4),
+                              "d2h_s": round(R[api.B200_PRM_R_TIME_D2H], 4)})
     return out
 
 
@@ -1104,7 +1111,8 @@ def main_ours(args, world, rank, local):
     asm = device_assembly_c2(lib, args.n, b)
 
     # e2e through monolis_solve_R with pinned host buffers (matrix upload included)
-    e2e64 = e2e_calls(m, b, n_unk, 0, args.steps)
+    e2e64_parts = []
+    e2e64 = e2e_calls(m, b, n_unk, 0, args.steps, e2e64_parts)
     e2e32 = e2e_calls(m, b, n_unk, 1, min(args.steps, 5))
     h2d = nz * nd * nd * 8 + nz * 4 + (N + 1) * 4 + n_unk * 8  # values, items, offsets, b
     d2h = n_unk * 8
@@ -1222,7 +1230,7 @@ def main_ours(args, world, rank, local):
             "spmv_layout": layout,
             "e2e": {"value": e2e64_max, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "monolis_solve_R (FP64), pinned host b/x, matrix uploaded every call",
-                    "statistic": f"mean of {len(e2e64)} calls", **stats(e2e64)},
+                    "statistic": f"mean of {len(e2e64)} calls", **stats(e2e64), "calls": e2e64_parts},
             "gpu_launches": launches,
             "autotuned_unroll": {"fp64": u64, "fp32": u32},
             "clocks": clocks,
