@@ -918,9 +918,10 @@ static bool sharded_supported(const MONOLIS* m) {
   const int mth = I[MONOLIS_PRM_I_METHOD];
   if ((mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG &&
        mth != MONOLIS_ITER_GROPCG) ||
-      (I[MONOLIS_B200_PRM_I_PRECISION] != 0 && mth != MONOLIS_ITER_CG)) {
+      (I[MONOLIS_B200_PRM_I_PRECISION] != 0 && mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB)) {
     fprintf(stderr,
-            "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG\n");
+            "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG or "
+            "BiCGSTAB\n");
     return false;
   }
   return true;

@@ -661,13 +661,15 @@ __global__ void shard_grop_kernel(SolverState* st, double* hist) {
 // ---------------------------------------------------------------------------
 // P = R + beta*(P - omega*V) (or P = R on iteration 1); PT = M^-1 P.
 // Mixed precision (x64 != null): after a refresh it also folds the FP32
-// correction into the FP64 solution, X += Y, Y = 0. Register-blocked like
-// cg_update_kernel (the work vectors are the solver's own, 16-byte aligned).
+// correction into the FP64 solution, X += Y, Y = 0, on the ghost entries
+// [N*B, n_ext) as well (several ranks: the owners' arithmetic, so the
+// refresh can multiply x + y there). Register-blocked like cg_update_kernel
+// (the work vectors are the solver's own, 16-byte aligned).
 template <int B, class T>
 __global__ void __launch_bounds__(kThreads)
     bicg_p_kernel(int N, T* __restrict__ p, const T* __restrict__ r, const T* __restrict__ vv,
                   T* __restrict__ pt, const T* __restrict__ alu, int prec, const SolverState* st,
-                  double* __restrict__ x64 = nullptr, T* __restrict__ yacc = nullptr) {
+                  double* __restrict__ x64 = nullptr, T* __restrict__ yacc = nullptr, long long n_ext = 0) {
   using RG = RowGroup<T, B>;
   constexpr int R = RG::R, E = RG::E;
   if (st->done) return;
@@ -722,6 +724,11 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int c = 0; c < B; c++) pt[row * B + c] = w[c];
   }
+  if (fold)
+    for (long long i = (long long)N * B + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n_ext; i += stride) {
+      x64[i] += (double)yacc[i];
+      yacc[i] = (T)0;
+    }
 }
 
 // V = A PT; c2 = <RT,V>; alpha = rho/c2 (BiCGSTAB.f90:113-123)
@@ -823,13 +830,16 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks<B>::value)
 
 // X = X + alpha*PT + omega*ST; R = -omega*T + S; <R,R>, <R,RT>
 // (BiCGSTAB.f90:148-164). On iter % iter_RR == 0 only X is updated here.
+// n_ghost entries after the owned ones get the X update too (the FP32
+// correction of the multi-rank refined solve, kept with the owners'
+// arithmetic; PT and ST hold their ghost entries after the halo updates).
 __device__ void fin_mixed_bicg(SolverState* st, double rr, double rrt, double* hist);
 
 template <int B, class T, bool Mixed = false>
 __global__ void __launch_bounds__(kThreads)
     bicg_xr_kernel(int N, T* __restrict__ x, const T* __restrict__ pt, const T* __restrict__ stv,
                    T* __restrict__ r, const T* __restrict__ s, const T* __restrict__ t, const T* __restrict__ rt,
-                   double* partials, unsigned int* ticket, SolverState* st, double* hist) {
+                   double* partials, unsigned int* ticket, SolverState* st, double* hist, long long n_ghost) {
   constexpr int W = Vec16T<T>::n;  // elements per 16-byte access
   if (st->done) return;
   const bool rr_iter = (st->iter % st->iter_rr) == 0;
@@ -862,6 +872,8 @@ __global__ void __launch_bounds__(kThreads)
       vstore<T, W>(r + i0, tv);
     }
   }
+  for (long long i = n + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n + n_ghost; i += stride)
+    x[i] = add_rn(add_rn(x[i], mul_rn(alpha, pt[i])), mul_rn(omega, stv[i]));
   for (long long i = nv * W + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += stride) {
     x[i] = add_rn(add_rn(x[i], mul_rn(alpha, pt[i])), mul_rn(omega, stv[i]));
     if (!rr_iter) {
@@ -876,7 +888,7 @@ __global__ void __launch_bounds__(kThreads)
     return;
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
-    if (!Mixed && st->sharded) {  // fin_bicg after the all-reduce (shard_bicg_kernel)
+    if (st->sharded) {  // fin_bicg / fin_mixed_bicg after the all-reduce (shard_bicg_kernel, shard_mbicg_kernel)
       st->red[0] = tot[0];
       st->red[1] = tot[1];
       return;
@@ -982,6 +994,10 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks2<B>::value)
     }
   }
   grid_reduce<1>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // alpha after the all-reduce (shard_mbicg_alpha_kernel)
+      st->red[0] = tot[0];
+      return;
+    }
     st->c2 = tot[0];
     st->fold = 0;  // the p kernel of this iteration has folded y
     if (tot[0] == 0.0) { st->done = 1; st->status = kBreakdown; return; }
@@ -1015,10 +1031,29 @@ __global__ void __launch_bounds__(kThreads, SpmvMinBlocks2<B>::value)
     }
   }
   grid_reduce<2>(v, partials, ticket, [&](double* tot) {
+    if (st->sharded) {  // omega after the all-reduce (shard_bicg_omega_kernel)
+      st->red[0] = tot[0];
+      st->red[1] = tot[1];
+      return;
+    }
     st->ts = tot[0];
     st->tt = tot[1];
     st->omega = tot[1] == 0.0 ? 0.0 : tot[0] / tot[1];
   });
+}
+
+// Multi-rank FP32-refined BiCGSTAB: the scalar steps with the all-reduced
+// sums in red[] (omega: shard_bicg_omega_kernel).
+__global__ void shard_mbicg_alpha_kernel(SolverState* st) {
+  if (st->done) return;
+  st->c2 = st->red[0];
+  st->fold = 0;
+  if (st->red[0] == 0.0) { st->done = 1; st->status = kBreakdown; return; }
+  st->alpha = st->rho / st->red[0];
+}
+__global__ void shard_mbicg_kernel(SolverState* st, double* hist) {
+  if (st->done) return;
+  fin_mixed_bicg(st, st->red[0], st->red[1], hist);
 }
 
 // P = Z + beta*P in FP32 (P = Z on iteration 1), and after a refresh the
@@ -1243,9 +1278,10 @@ __global__ void shard_mixed_inner_kernel(SolverState* st, double* hist) {
   if (st->done) return;
   fin_mixed_inner(st, st->red[0], st->red[1], hist);
 }
+template <bool Bicg>
 __global__ void shard_mixed_refresh_kernel(SolverState* st, double* hist) {
   if (st->done || !(st->iter == 0 || st->refresh)) return;
-  fin_mixed_refresh<false>(st, st->red[0], st->red[1], hist);
+  fin_mixed_refresh<Bicg>(st, st->red[0], st->red[1], hist);
 }
 
 // Refresh: r64 = b - A64 (x + y) with the FP64 matrix, r = fp32(r64),
@@ -1412,8 +1448,10 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     fprintf(stderr, "** monolis_b200: GropCG and PipeCG run in FP64\n");
     return kBadInput;
   }
-  if (p.shard && ((p.precision != 0 && p.method != 1) || p.np_rows < N)) {
-    fprintf(stderr, "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG\n");
+  if (p.shard && ((p.precision != 0 && p.method != 1 && p.method != 5) || p.np_rows < N)) {
+    fprintf(stderr,
+            "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG or "
+            "BiCGSTAB\n");
     return kBadInput;
   }
   // vectors gathered by the SpMV hold the ghost rows too
@@ -1744,7 +1782,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           shard_allreduce(*sp, st->red, 2, ss);
           shard_bicg_omega_kernel<<<1, 1, 0, ss>>>(st);
           if (ev) cudaEventRecord(ev[4], ss);
-          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist, 0);
           if (!special) {
             shard_allreduce(*sp, st->red, 2, ss);
             shard_bicg_kernel<<<1, 1, 0, ss>>>(st, hist);
@@ -1782,13 +1820,78 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
           if (ev) cudaEventRecord(ev[3], ss);
           k_t<<<g_t, kThreads, 0, ss>>>(A64, stv, t, sv, partials, ticket, st, RowSet{nullptr, 0}, 0);
           if (ev) cudaEventRecord(ev[4], ss);
-          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+          k_xr<<<g_xr, kThreads, 0, ss>>>(N, x, pt, stv, r, sv, t, rt, partials, ticket, st, hist, 0);
           if (ev) cudaEventRecord(ev[5], ss);
           if (special) k_resid<<<g_resid, kThreads, 0, ss>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket,
                                                              st, hist);
           if (ev) cudaEventRecord(ev[6], ss);
         };
       }
+    } else if (p.method == 5 && p.shard) {
+      // multi-rank FP32-refined BiCGSTAB: FP32 halo updates of PT and ST
+      // before the products, every dot product all-reduced, the refresh's
+      // all-reduce in every iteration (the refresh is decided on the device,
+      // from all-reduced sums, identically on every rank). The ghost entries
+      // of y (y += alpha PT + omega ST after both halo updates) and of x (the
+      // folds) follow the owners' arithmetic, so the FP64 refresh multiplies
+      // x + y on the ghost rows without a halo update of its own.
+      const ShardPlan* sp = p.shard;
+      SellView2 A32 = view2_of(m);
+      const float* alu32 = m.d_alu32;
+      float *r = vec.get<float>(n), *rt = vec.get<float>(n), *pp = vec.get<float>(n),
+            *pt = vec.get<float>(n_ext), *sv = vec.get<float>(n), *stv = vec.get<float>(n_ext),
+            *t = vec.get<float>(n), *vv = vec.get<float>(n), *y = vec.get<float>(n_ext);
+      if (!r || !rt || !pp || !pt || !sv || !stv || !t || !vv || !y) return kCudaError;
+      double* x = d_x;
+      const double* b = d_b;
+      auto k_v = mbicg_v_kernel<B, U>;
+      auto k_t = mbicg_t_kernel<B, U>;
+      auto k_xr = bicg_xr_kernel<B, float, true>;
+      auto k_ref = mixed_refresh_kernel<B, U, true>;
+      const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr), g_ref = pgrid(k_ref);
+      const int g_p = pgrid(bicg_p_kernel<B, float>), g_s = pgrid(bicg_s_kernel<B, float>);
+      if (cudaMemsetAsync(y, 0, sizeof(float) * n_ext, s) != cudaSuccess ||
+          cudaMemsetAsync(pt, 0, sizeof(float) * n_ext, s) != cudaSuccess ||
+          cudaMemsetAsync(stv, 0, sizeof(float) * n_ext, s) != cudaSuccess)
+        return kCudaError;
+      int rc2 = shard_halo(*sp, x, s);
+      k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
+      if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
+      shard_mixed_refresh_kernel<true><<<1, 1, 0, s>>>(st, hist);
+      if (rc2) return rc2;
+      const int hk = (sp->n_send > 0) + (sp->n_recv > 0);  // pack / unpack kernels of a halo update
+      const long long n_ghost = n_ext - n;
+      plan.kernels = 6;
+      plan.always_all = true;
+      plan.launches = 10 + 2 * hk;
+      plan.launches_special = plan.launches;
+      plan.kind = {2, 0, 2, 0, 1, 0};
+      plan.iteration = [=](cudaStream_t ss, cudaEvent_t* ev, bool) {
+        if (ev) cudaEventRecord(ev[0], ss);
+        bicg_p_kernel<B, float><<<g_p, kThreads, 0, ss>>>(N, pp, r, vv, pt, alu32, prec, st, x, y, n_ext);
+        if (ev) cudaEventRecord(ev[1], ss);
+        shard_halo(*sp, pt, ss);
+        k_v<<<g_v, kThreads, 0, ss>>>(A32, pt, vv, rt, partials, ticket, st);
+        shard_allreduce(*sp, st->red, 1, ss);
+        shard_mbicg_alpha_kernel<<<1, 1, 0, ss>>>(st);
+        if (ev) cudaEventRecord(ev[2], ss);
+        bicg_s_kernel<B, float><<<g_s, kThreads, 0, ss>>>(N, sv, r, vv, stv, alu32, prec, st);
+        if (ev) cudaEventRecord(ev[3], ss);
+        shard_halo(*sp, stv, ss);
+        k_t<<<g_t, kThreads, 0, ss>>>(A32, stv, t, sv, partials, ticket, st);
+        shard_allreduce(*sp, st->red, 2, ss);
+        shard_bicg_omega_kernel<<<1, 1, 0, ss>>>(st);
+        if (ev) cudaEventRecord(ev[4], ss);
+        k_xr<<<g_xr, kThreads, 0, ss>>>(N, y, pt, stv, r, sv, t, rt, partials, ticket, st, hist, n_ghost);
+        shard_allreduce(*sp, st->red, 2, ss);
+        shard_mbicg_kernel<<<1, 1, 0, ss>>>(st, hist);
+        if (ev) cudaEventRecord(ev[5], ss);
+        k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
+        shard_allreduce(*sp, st->red, 2, ss);
+        shard_mixed_refresh_kernel<true><<<1, 1, 0, ss>>>(st, hist);
+        if (ev) cudaEventRecord(ev[6], ss);
+      };
+      plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n_ext, x, y, st); };
     } else if (p.method == 5) {
       SellView2 A32 = view2_of(m);
       const float* alu32 = m.d_alu32;
@@ -1819,7 +1922,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (ev) cudaEventRecord(ev[3], ss);
         k_t<<<g_t, kThreads, 0, ss>>>(A32, stv, t, sv, partials, ticket, st);
         if (ev) cudaEventRecord(ev[4], ss);
-        k_xr<<<g_xr, kThreads, 0, ss>>>(N, y, pt, stv, r, sv, t, rt, partials, ticket, st, hist);
+        k_xr<<<g_xr, kThreads, 0, ss>>>(N, y, pt, stv, r, sv, t, rt, partials, ticket, st, hist, 0);
         if (ev) cudaEventRecord(ev[5], ss);
         k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
         if (ev) cudaEventRecord(ev[6], ss);
@@ -1851,7 +1954,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       int rc2 = shard_halo(*sp, x, s);
       k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
       if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
-      shard_mixed_refresh_kernel<<<1, 1, 0, s>>>(st, hist);
+      shard_mixed_refresh_kernel<false><<<1, 1, 0, s>>>(st, hist);
       if (rc2) return rc2;
       const int hk = (sp->n_send > 0) + (sp->n_recv > 0);
       plan.kernels = 4;
@@ -1874,7 +1977,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (ev) cudaEventRecord(ev[3], ss);
         k_ref<<<g_ref, kThreads, 0, ss>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
         shard_allreduce(*sp, st->red, 2, ss);
-        shard_mixed_refresh_kernel<<<1, 1, 0, ss>>>(st, hist);
+        shard_mixed_refresh_kernel<false><<<1, 1, 0, ss>>>(st, hist);
         if (ev) cudaEventRecord(ev[4], ss);
       };
       plan.finalize = [=](cudaStream_t ss) { mixed_fold_kernel<<<gvec, kThreads, 0, ss>>>(n_ext, x, y, st); };

@@ -1,6 +1,7 @@
 """The multi-rank device path (halo updates through NCCL, dot products summed
 by an NCCL all-reduce, scalar updates in separate one-thread kernels), FP64
-CG, GropCG, PipeCG and BiCGSTAB, run with a one-rank communicator: it must give exactly the
+CG, GropCG, PipeCG and BiCGSTAB and FP32-refined CG and BiCGSTAB, run with a
+one-rank communicator: it must give exactly the
 bits and iteration count of the single-rank solve, also past the
 true-residual replacement at iteration 200. (Runs here have one GPU; more
 ranks cannot share it.)"""
@@ -63,8 +64,8 @@ def test_sharded_path_rejects_unsupported(gpu):
     ms.set_error_abort(False)
     ms.set_halo(p, 0, 1)
     ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
-    _, _, _, st = solve(ms, b, api.ITER_BICGSTAB, api.PREC_DIAG, precision=1)
-    assert st == 5  # on several ranks the FP32-refined form is CG only
+    _, _, _, st = solve(ms, b, api.ITER_PIPECG, api.PREC_DIAG, precision=1)
+    assert st == 5  # the FP32-refined form is CG and BiCGSTAB only
     ms.finalize()
 
 
@@ -195,6 +196,101 @@ def test_sharded_mixed_cg_one_rank_bit_identical(gpu, problem, kw, tol):
     assert sts == 0
     assert its == itp and ress == resp and ms.Iarray[api.B200_PRM_I_N_REFINE] == nref
     assert bits_equal(xs, xp)
+    ms.finalize()
+
+
+@pytest.mark.parametrize("problem,kw,tol", [
+    ("convection_diffusion", dict(n=16, peclet=5.0), 1e-8),
+    ("convection_diffusion", dict(n=20, peclet=50.0), 1e-9),
+    ("laplacian", dict(n=18), 1e-10),
+    ("elasticity", dict(n=9), 1e-8),
+])
+def test_sharded_mixed_bicgstab_one_rank_bit_identical(gpu, problem, kw, tol):
+    """The multi-rank FP32-refined BiCGSTAB (FP32 halo updates of PT and ST,
+    all-reduced dot products, the refresh's all-reduce in every iteration,
+    y and x kept on the ghost rows) through a one-rank NCCL communicator:
+    the iteration count, residual, refresh count and solution bits of the
+    plain refined solve."""
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    xp, itp, resp, stp = solve(mp, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=tol, precision=1)
+    assert stp == 0 and resp < tol
+    nref = mp.Iarray[api.B200_PRM_I_N_REFINE]
+    assert nref >= 1
+    p = partition.partition_rank(mp.csr_index(), mp.csr_item() - 1, mp.values(), nd, 1, 0)
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(p["N"], p["NP"], nd, len(p["item"]), p["val"], p["index"], p["item"])
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_halo(p, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    xs, its, ress, sts = solve(ms, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=tol, precision=1)
+    assert sts == 0
+    assert its == itp and ress == resp and ms.Iarray[api.B200_PRM_I_N_REFINE] == nref
+    assert bits_equal(xs, xp)
+    ms.finalize()
+
+
+def _mirrored_system(mp, every=7, first=3):
+    """The system of mp with the columns of every `every`-th node (from
+    `first`) read through a ghost copy filled by a one-rank self-exchange:
+    (N, NP, index, item, val, halo, mirrored)."""
+    nd = mp.NDOF
+    N = mp.N
+    index = mp.csr_index().astype(np.int64)
+    item = (mp.csr_item() - 1).astype(np.int64)
+    val = mp.values().reshape(-1, nd * nd)
+    mirrored = np.arange(first, N, every)
+    ghost = np.full(N, -1, dtype=np.int64)
+    ghost[mirrored] = N + np.arange(len(mirrored))
+    NP = N + len(mirrored)
+    new_index, new_item, new_val = [0], [], []
+    for i in range(N):
+        cols = item[index[i]:index[i + 1]]
+        cols2 = np.where((ghost[cols] >= 0) & (cols != i), ghost[cols], cols)
+        order = np.argsort(cols2, kind="stable")
+        new_item.extend(cols2[order].tolist())
+        new_val.append(val[index[i]:index[i + 1]][order])
+        new_index.append(len(new_item))
+    new_index += [new_index[-1]] * (NP - N)
+    new_val = np.concatenate(new_val).reshape(-1)
+    halo = {"N": N, "recv_pe": [0], "recv_index": [0, len(mirrored)], "recv_item": np.arange(N, NP),
+            "send_pe": [0], "send_index": [0, len(mirrored)], "send_item": mirrored}
+    return (N, NP, np.array(new_index, dtype=np.int32), np.array(new_item, dtype=np.int32), new_val, halo,
+            mirrored)
+
+
+@pytest.mark.parametrize("problem,kw", [("convection_diffusion", dict(n=14, peclet=5.0)),
+                                        ("laplacian", dict(n=14))])
+def test_sharded_mixed_bicgstab_through_self_halo(gpu, problem, kw):
+    """FP32-refined BiCGSTAB on a one-rank system whose rows read every 7th
+    node through a ghost copy (filled by a self-exchange): PT and ST cross
+    the halo in FP32, the FP64 refreshes multiply x + y on the ghost rows,
+    which the solver keeps with the owners' arithmetic; the solution reaches
+    the tolerance on the FP64 residual of the original system and matches
+    the plain refined solve to it."""
+    mp, b = build(gpu, problem, **kw)
+    nd = mp.NDOF
+    tol = 1e-9
+    x_ref, it_ref, _, st = solve(mp, b, api.ITER_BICGSTAB, api.PREC_DIAG, tol=tol, precision=1)
+    assert st == 0
+    N, NP, index, item, val, halo, mirrored = _mirrored_system(mp)
+    ms = api.Monolis(gpu)
+    ms.set_matrix_BCSR(N, NP, nd, len(item), val, index, item)
+    ms.quiet()
+    ms.set_error_abort(False)
+    ms.set_halo(halo, 0, 1)
+    ms.com_init_nccl(api.nccl_unique_id(gpu), 0, 1)
+    bl = np.zeros(NP * nd)
+    bl[:N * nd] = b
+    xs, its, ress, sts = solve(ms, bl, api.ITER_BICGSTAB, api.PREC_DIAG, tol=tol, precision=1)
+    assert sts == 0 and ress < tol
+    assert ms.Iarray[api.B200_PRM_I_N_REFINE] >= 1
+    x = xs[:N * nd]
+    assert np.linalg.norm(b - mp.matvec(x)) / np.linalg.norm(b) < 1.01 * tol
+    assert abs(its - it_ref) <= max(5, it_ref // 5), (its, it_ref)
+    assert np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref) < 1e-6
+    assert bits_equal(xs[N * nd:].reshape(-1, nd), xs[:N * nd].reshape(-1, nd)[mirrored])
     ms.finalize()
 
 
