@@ -1440,6 +1440,11 @@ int largest_divisor_at_most(int v, int cap) {
 int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double* d_b, double* d_x,
                  SolveResult& res, double* h_hist, cudaStream_t s) {
   const int N = m.N, nd = m.ndof;
+  // Grids: a kernel's persistent grid, or one block per 256 rows when the
+  // system is smaller than that, so a small system does not pay for entering
+  // and reducing hundreds of idle blocks.
+  const int gcap = (int)std::max<long long>(1, ((long long)N + kThreads - 1) / kThreads);
+  auto pg = [gcap](auto k) { return std::min(pgrid(k), gcap); };
   const long long n = (long long)N * nd;
   const int prec = p.precond == 1 ? 1 : 0;
   if (prec && !m.have_alu) return kBadInput;
@@ -1509,13 +1514,13 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
     unsigned int* ticket = sc.ticket;
     SolverState* st = sc.st;
     double* hist = sc.hist;
-    const int gvec = num_sms() * 8;
+    const int gvec = (int)std::min<long long>(num_sms() * 8, std::max<long long>(1, (n + kThreads - 1) / kThreads));
     if (p.precision == 0) {
       const double* alu = m.d_alu64;
       double* x = d_x;
       const double* b = d_b;
       auto k_resid = resid_kernel<B, U, double, double>;
-      const int g_resid = pgrid(k_resid);
+      const int g_resid = pg(k_resid);
       if (p.method == 1 && p.shard) {
         // multi-rank CG: halo updates before the products, all-reduced dots
         const ShardPlan* sp = p.shard;
@@ -1525,7 +1530,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (cudaMemsetAsync(pp, 0, sizeof(double) * n_ext, s) != cudaSuccess) return kCudaError;
         auto k_spmv = cg_spmv_kernel<B, U, double, double, true>;
         auto k_upd = cg_update_kernel<B, double>;
-        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+        const int g_spmv = pg(k_spmv), g_upd = pg(k_upd);
         int rc2 = shard_halo(*sp, x, s);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
         if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
@@ -1577,7 +1582,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_upd = grop_update_kernel<double>;
         auto k_mvps = grop_spmv_kernel<B, U, double, double>;
         auto k_mv = pipe_spmv_kernel<B, U, double, double>;
-        const int g_q = pgrid(k_q), g_upd = pgrid(k_upd), g_mvps = pgrid(k_mvps), g_mv = pgrid(k_mv);
+        const int g_q = pg(k_q), g_upd = pg(k_upd), g_mvps = pg(k_mvps), g_mv = pg(k_mv);
         // R = B - A X, U = M^-1 R, B2 and gamma = <R,U> (CG's initial step);
         // P = U, S = A P (GropCG.f90:67-86)
         int rc2 = sp ? shard_halo(*sp, x, s) : kOk;
@@ -1634,7 +1639,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_dots = pipe_dots_kernel<B, double>;
         auto k_mv = pipe_spmv_kernel<B, U, double, double>;
         auto k_upd = pipe_update_kernel<double>;
-        const int g_dots = pgrid(k_dots), g_mv = pgrid(k_mv), g_upd = pgrid(k_upd);
+        const int g_dots = pg(k_dots), g_mv = pg(k_mv), g_upd = pg(k_upd);
         int rc2 = shard_halo(*sp, x, s);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st, hist);
         if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
@@ -1688,7 +1693,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_dots = pipe_dots_kernel<B, double>;
         auto k_mv = pipe_spmv_kernel<B, U, double, double>;
         auto k_upd = pipe_update_kernel<double>;
-        const int g_dots = pgrid(k_dots), g_mv = pgrid(k_mv), g_upd = pgrid(k_upd);
+        const int g_dots = pg(k_dots), g_mv = pg(k_mv), g_upd = pg(k_upd);
         // R = B - A X, U = M^-1 R, B2 (PipeCG.f90:67-83); V = A U
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, u, nullptr, alu, prec, 2, partials, ticket, st, hist);
         k_mv<<<g_mv, kThreads, 0, s>>>(A64, u, vv, st);
@@ -1715,7 +1720,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         if (!r || !z || !q || !pp) return kCudaError;
         auto k_spmv = cg_spmv_kernel<B, U, double, double>;
         auto k_upd = cg_update_kernel<B, double>;
-        const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
+        const int g_spmv = pg(k_spmv), g_upd = pg(k_upd);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, z, nullptr, alu, prec, 0, partials, ticket, st, hist);
         plan.kernels = 4;
         plan.kind = {1, 0, 2, 0};
@@ -1745,8 +1750,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_v = bicg_v_kernel<B, U, double, double, true>;
         auto k_t = bicg_t_kernel<B, U, double, double, true>;
         auto k_xr = bicg_xr_kernel<B, double>;
-        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
-        const int g_p = pgrid(bicg_p_kernel<B, double>), g_s = pgrid(bicg_s_kernel<B, double>);
+        const int g_v = pg(k_v), g_t = pg(k_t), g_xr = pg(k_xr);
+        const int g_p = pg(bicg_p_kernel<B, double>), g_s = pg(bicg_s_kernel<B, double>);
         int rc2 = shard_halo(*sp, x, s);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
         if (!rc2) rc2 = shard_allreduce(*sp, st->red, 2, s);
@@ -1805,8 +1810,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
         auto k_v = bicg_v_kernel<B, U, double, double>;
         auto k_t = bicg_t_kernel<B, U, double, double>;
         auto k_xr = bicg_xr_kernel<B, double>;
-        const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr);
-        const int g_p = pgrid(bicg_p_kernel<B, double>), g_s = pgrid(bicg_s_kernel<B, double>);
+        const int g_v = pg(k_v), g_t = pg(k_t), g_xr = pg(k_xr);
+        const int g_p = pg(bicg_p_kernel<B, double>), g_s = pg(bicg_s_kernel<B, double>);
         k_resid<<<g_resid, kThreads, 0, s>>>(A64, x, b, r, nullptr, rt, alu, prec, 1, partials, ticket, st, hist);
         plan.kernels = 6;
         plan.kind = {2, 0, 2, 0, 1, 0};
@@ -1848,8 +1853,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_t = mbicg_t_kernel<B, U>;
       auto k_xr = bicg_xr_kernel<B, float, true>;
       auto k_ref = mixed_refresh_kernel<B, U, true>;
-      const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr), g_ref = pgrid(k_ref);
-      const int g_p = pgrid(bicg_p_kernel<B, float>), g_s = pgrid(bicg_s_kernel<B, float>);
+      const int g_v = pg(k_v), g_t = pg(k_t), g_xr = pg(k_xr), g_ref = pg(k_ref);
+      const int g_p = pg(bicg_p_kernel<B, float>), g_s = pg(bicg_s_kernel<B, float>);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n_ext, s) != cudaSuccess ||
           cudaMemsetAsync(pt, 0, sizeof(float) * n_ext, s) != cudaSuccess ||
           cudaMemsetAsync(stv, 0, sizeof(float) * n_ext, s) != cudaSuccess)
@@ -1905,8 +1910,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_t = mbicg_t_kernel<B, U>;
       auto k_xr = bicg_xr_kernel<B, float, true>;
       auto k_ref = mixed_refresh_kernel<B, U, true>;
-      const int g_v = pgrid(k_v), g_t = pgrid(k_t), g_xr = pgrid(k_xr), g_ref = pgrid(k_ref);
-      const int g_p = pgrid(bicg_p_kernel<B, float>), g_s = pgrid(bicg_s_kernel<B, float>);
+      const int g_v = pg(k_v), g_t = pg(k_t), g_xr = pg(k_xr), g_ref = pg(k_ref);
+      const int g_p = pg(bicg_p_kernel<B, float>), g_s = pg(bicg_s_kernel<B, float>);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
       k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, nullptr, alu32, prec, partials, ticket, st, hist, rt);
       plan.kernels = 6;
@@ -1948,7 +1953,7 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_spmv = cg_spmv2_kernel<B, U>;
       auto k_upd = mixed_update_kernel<B>;
       auto k_ref = mixed_refresh_kernel<B, U>;
-      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd), g_ref = pgrid(k_ref);
+      const int g_spmv = pg(k_spmv), g_upd = pg(k_upd), g_ref = pg(k_ref);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n_ext, s) != cudaSuccess) return kCudaError;
       if (cudaMemsetAsync(pp, 0, sizeof(float) * n_ext, s) != cudaSuccess) return kCudaError;
       int rc2 = shard_halo(*sp, x, s);
@@ -1992,8 +1997,8 @@ int solve_device(SellMatrix& m, Scratch& sc, const SolveParams& p, const double*
       auto k_spmv = cg_spmv2_kernel<B, U>;
       auto k_upd = mixed_update_kernel<B>;
       auto k_ref = mixed_refresh_kernel<B, U>;
-      const int g_spmv = pgrid(k_spmv), g_upd = pgrid(k_upd);
-      const int g_ref = pgrid(k_ref);
+      const int g_spmv = pg(k_spmv), g_upd = pg(k_upd);
+      const int g_ref = pg(k_ref);
       if (cudaMemsetAsync(y, 0, sizeof(float) * n, s) != cudaSuccess) return kCudaError;
       k_ref<<<g_ref, kThreads, 0, s>>>(A64, x, y, b, r, z, alu32, prec, partials, ticket, st, hist, nullptr);
       plan.kernels = 4;
