@@ -916,12 +916,14 @@ static void* nccl_comm_of(MONOLIS_COM* com) {
 static bool sharded_supported(const MONOLIS* m) {
   const int* I = m->prm.Iarray;
   const int mth = I[MONOLIS_PRM_I_METHOD];
-  if ((mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB && mth != MONOLIS_ITER_PIPECG &&
-       mth != MONOLIS_ITER_GROPCG) ||
-      (I[MONOLIS_B200_PRM_I_PRECISION] != 0 && mth != MONOLIS_ITER_CG && mth != MONOLIS_ITER_BICGSTAB)) {
+  // BiCGSTAB_N128 runs as BiCGSTAB (its dot products are double-double on
+  // every rank; the ranks' partial sums are rounded before the all-reduce)
+  const bool bicg = mth == MONOLIS_ITER_BICGSTAB || mth == MONOLIS_ITER_BICGSTAB_N128;
+  if ((mth != MONOLIS_ITER_CG && !bicg && mth != MONOLIS_ITER_PIPECG && mth != MONOLIS_ITER_GROPCG) ||
+      (I[MONOLIS_B200_PRM_I_PRECISION] != 0 && mth != MONOLIS_ITER_CG && !bicg)) {
     fprintf(stderr,
-            "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB) or FP32-refined CG or "
-            "BiCGSTAB\n");
+            "** monolis_b200: the multi-rank solve is FP64 (CG, GropCG, PipeCG, BiCGSTAB, BiCGSTAB_N128) or "
+            "FP32-refined CG or BiCGSTAB\n");
     return false;
   }
   return true;

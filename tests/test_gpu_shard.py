@@ -26,6 +26,7 @@ pytestmark = pytest.mark.gpu
     ("elasticity", dict(n=12), api.ITER_PIPECG, 0),
     ("laplacian", dict(n=20), api.ITER_PIPECG, 9),
     ("elasticity", dict(n=12), api.ITER_GROPCG, 0),
+    ("convection_diffusion", dict(n=16, peclet=50.0), api.ITER_BICGSTAB_N128, 0),
 ])
 def test_sharded_path_one_rank_bit_identical(gpu, problem, kw, method, rr):
     """rr > 0: true residual every rr iterations (instead of 200), so the
